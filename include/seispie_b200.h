@@ -1,0 +1,174 @@
+/*
+ * seispie_b200.h -- C ABI of the B200 (sm_100a) FWI solver library
+ * libseispie_b200.so.
+ *
+ * The library replaces the Numba @cuda.jit kernels and device-side time loops
+ * of icui/seispie's fd2d solver plugin (seispie/solver/fd2d/solver.py,
+ * seispie/solver/fd2d/fd2d.py, seispie/solver/misfit/waveform.py,
+ * seispie/solver/source/ricker.py).  Each entry point below names the
+ * reference code it replaces.  All paths in citations are relative to the
+ * seispie project root.
+ *
+ * Conventions
+ *   - Every pointer argument is a DEVICE pointer unless stated otherwise.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ *     stream).  All work is enqueued on it; nothing synchronises the host.
+ *   - Every function returns 0 on success or a negative FWI_E* code; the
+ *     message of the last failure on the calling thread is available from
+ *     fwi_last_error().  No function allocates device memory: every buffer,
+ *     scratch included, is owned by the caller.
+ *   - Wavefield layout: z is contiguous.  A field of one shot is nx rows of
+ *     `pitch` floats (pitch >= nz, pitch % 4 == 0, cells [nz, pitch) of a row
+ *     are padding that must be zero and stay zero).  A batch stores its shots
+ *     back to back: element (shot, i, j) is at shot*nx*pitch + i*pitch + j.
+ *     Point positions (sources, receivers) use the reference's cell number
+ *     k = i*nz + j (fd2d.py:134, 159).
+ */
+#ifndef SEISPIE_B200_H
+#define SEISPIE_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FWI_ABI_VERSION 1
+
+/* status codes */
+#define FWI_OK 0
+#define FWI_EINVAL (-1)   /* bad argument (null pointer, size, alignment)   */
+#define FWI_ECUDA (-2)    /* a CUDA runtime call or kernel launch failed     */
+#define FWI_ERANGE (-3)   /* size beyond a documented maximum                */
+
+/* wave types, solver.py:205-234 */
+#define FWI_SH 0          /* SH: vy, uy, sxy, szy                            */
+#define FWI_PSV 1         /* P-SV: vx, vz, ux, uz, sxx, szz, sxz             */
+#define FWI_SPIN 2        /* P-SV plus micropolar spin vy_c, uy_c, sy*_c     */
+
+/*
+ * One batch of shots that share a model and a grid.  Field slots:
+ *   sig[2][6]  stress, ping-pong pair; SH: {sxy, szy}; P-SV: {sxx, szz, sxz};
+ *              spin adds {syx_c, syy_c, syz_c} in slots 3..5
+ *   vel[2][3]  velocity, ping-pong pair; SH: {vy}; P-SV: {vx, vz};
+ *              spin adds vy_c in slot 2
+ *   disp[3]    displacement, updated in place, same slots as vel
+ * `cur` selects which half of each pair holds the current state; fwi_run
+ * flips it once per step.
+ * Model (shared by all shots, [nx][pitch]; prepared by fwi_prepare_model):
+ *   buo = dt/rho, buo_j = dt/j (spin), bound (sponge), lam, mu,
+ *   nu, mnc = mu_c + nu_c (spin).
+ * Injection (per shot, CSR): the entries of shot s are inj_ptr[s] ..
+ *   inj_ptr[s+1]-1; entry e adds stf_c[inj_row[e]*nt + it] to the stress
+ *   divergence of component c at cell inj_cell[e] (reference numbering)
+ *   before the velocity update, in entry order (stf_dsy / stf_dsxz,
+ *   solver.py:78-93).  Component pointers: SH uses stf[1] (y); P-SV uses
+ *   stf[0] (x) and stf[2] (z).
+ * Receivers: rec_cell[nrec] (reference numbering), recorded into
+ *   obs[c][(shot*nrec + r)*nt + it] after each forward step (save_obs,
+ *   solver.py:151-156); obs[c] may be NULL to skip a component.
+ *   Components: SH obs[1] = uy; P-SV obs[0] = ux, obs[2] = uz;
+ *   spin also obs[1] = uy_c.
+ * Snapshots (forward; sae > 0): snap_u[c] is [nsa][nshots][nx][pitch]; slot
+ *   nsa-(it+1)/sae receives u as it is before step it whenever
+ *   (it+1) % sae == 0 (solver.py:193-203).  snap_v[c] (optional) receives v
+ *   after that step (solver.py:236-242).  NULL skips.
+ * Sensitivity kernels (adjoint; FP64, [nx][pitch], accumulated over every
+ *   shot of the batch): k_mu for SH (interaction_muy, solver.py:159-163,
+ *   315-321); k_lam, k_mu, k_rho for P-SV.  NULL skips.
+ */
+typedef struct fwi_batch {
+    int mode;                 /* FWI_SH, FWI_PSV or FWI_SPIN                 */
+    int nx, nz, pitch;        /* grid; pitch = padded z length               */
+    int nshots;               /* shots in this batch                         */
+    int nt;                   /* samples per source / receiver trace         */
+    float dx, dz;             /* grid spacing (fd2d.py:195-196)              */
+    double dt;                /* time step                                   */
+    int cur;                  /* current half of the ping-pong pairs (0/1)   */
+    int tile;                 /* tile variant (0 = library default)          */
+    float *sig[2][6];
+    float *vel[2][3];
+    float *disp[3];
+    const float *buo, *buo_j, *bound, *lam, *mu, *nu, *mnc;
+    const int *inj_ptr, *inj_cell, *inj_row;
+    const float *stf[3];
+    int nrec;
+    const int *rec_cell;
+    float *obs[3];
+    int sae, nsa;
+    float *snap_u[3];
+    float *snap_v[3];
+    double *k_lam, *k_mu, *k_rho;
+} fwi_batch;
+
+/* ABI version of the loaded library (FWI_ABI_VERSION). */
+int fwi_abi_version(void);
+
+/* Copy the last error message of the calling thread into buf (always NUL
+ * terminated); returns the status code of that error (0 if none). */
+int fwi_last_error(char *buf, size_t len);
+
+/* vp/vs -> lambda/mu in place: lam_io holds vp and mu_io holds vs on entry.
+ * Replaces vps2lm, seispie/solver/fd2d/fd2d.py:21-33 (launched at
+ * fd2d.py:216).  n elements, any layout. */
+int fwi_vps2lm(float *lam_io, float *mu_io, const float *rho, long long n, void *stream);
+
+/* lambda/mu -> vp/vs in place.  Replaces lm2vps, fd2d.py:36-44. */
+int fwi_lm2vps(float *vp_io, float *vs_io, const float *rho, long long n, void *stream);
+
+/* Gaussian sponge weights, [nx][pitch].  Replaces set_bound,
+ * fd2d.py:47-68 (launched at fd2d.py:225-228). */
+int fwi_set_bound(float *bound, int nx, int nz, int pitch, int width, double alpha,
+                  int left, int right, int bottom, int top, void *stream);
+
+/* Ricker source-time functions, FP64 arithmetic rounded to float32.
+ * params (device, nsrc x 4 doubles: f0, t0, ang [deg], amp) ->
+ * stf_x/stf_y/stf_z [nsrc*nt].  Replaces ricker, ricker.py:7-11, and the
+ * host loop of import_sources, fd2d.py:136-138. */
+int fwi_ricker(const double *params, int nsrc, int nt, double dt,
+               float *stf_x, float *stf_y, float *stf_z, void *stream);
+
+/* Derived per-cell model arrays used by fwi_run: buo = dt/rho,
+ * buo_j = dt/j, mnc = mu_c + nu_c (the last two only when j / mu_c are
+ * non-NULL).  n elements, any layout.  Replaces the per-step divisions of
+ * add_vy / add_vxz (solver.py:95-109) and the sum in add_sy_c
+ * (solver.py:140-141). */
+int fwi_prepare_model(const float *rho, const float *j, const float *mu_c, const float *nu_c,
+                      double dt, long long n, float *buo, float *buo_j, float *mnc, void *stream);
+
+/* Advance every shot of the batch by nsteps time steps starting at step it0.
+ * adjoint = 0: forward modelling; replaces the time loop of run_forward,
+ *   solver.py:192-242 (div_sy/div_sxz/div_sxyz_c, stf_dsy/stf_dsxz,
+ *   add_vy/add_vxz, div_vy/div_vxz, add_sy/add_sxz/add_sy_c, save_obs and
+ *   the snapshot copies), fused into one kernel launch per step.
+ * adjoint = 1: adjoint modelling; replaces run_adjoint, solver.py:290-321
+ *   (same step with the adjoint source, plus the interaction kernels every
+ *   sae steps with ndt = sae*dt).  Requires the forward snapshots.
+ * The caller clears the wavefields first (fwi_clear or cudaMemsetAsync),
+ * as clear_wavefields does (fd2d.py:318-341).  b->cur is updated. */
+int fwi_run(fwi_batch *b, int adjoint, int it0, int nsteps, void *stream);
+
+/* L2 waveform misfit and adjoint source for nshots x nrec traces of nt
+ * samples (receiver-major, [shot][rec][t]).  data = observed traces (the
+ * reference's `syn`), syn = synthetics (its `obs`).  Writes the
+ * time-reversed adjoint source adstf = 2 taper^2 (data - syn) and
+ * misfit[shot] = || taper (data - syn) ||_2 accumulated in FP64.
+ * partial is caller scratch of fwi_misfit_partials(nrec, nt) doubles per
+ * shot.  Replaces diff + waveform, seispie/solver/misfit/waveform.py:5-34. */
+int fwi_misfit(const float *data, const float *syn, float *adstf, double *misfit,
+               double *partial, int nshots, int nrec, int nt, double dt, void *stream);
+long long fwi_misfit_partials(int nrec, int nt);
+
+/* Separable Gaussian smoothing of an FP64 kernel ([nx][in_pitch]) into a
+ * float32 field ([nx][out_pitch]), normalised by the Gaussian mass inside
+ * the grid as init_gausian does; taps beyond 6 sigma (relative weight
+ * < 2e-8) are dropped.  tmp: caller scratch of nx*nz doubles.  sigma > 0.
+ * Replaces init_gausian / apply_gauxxian_x / apply_gauxxian_z and smooth,
+ * fd2d.py:76-108, 349-352. */
+int fwi_smooth(const double *in, int in_pitch, float *out, int out_pitch, double *tmp,
+               int nx, int nz, int sigma, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SEISPIE_B200_H */

@@ -1,0 +1,224 @@
+// extern "C" entry points of libseispie_b200.so (declared in
+// include/seispie_b200.h): argument checks, error reporting and the host
+// time loop that enqueues the fused step kernels.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "common.cuh"
+
+namespace fwi {
+
+static thread_local int g_code = 0;
+static thread_local char g_msg[512] = "";
+
+int set_error(int code, const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_msg, sizeof(g_msg), fmt, ap);
+    va_end(ap);
+    g_code = code;
+    return code;
+}
+
+int check_launch(const char *what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_error(FWI_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+    return 0;
+}
+
+// defined in step.cu / aux.cu
+int launch_step(const fwi_batch *b, int adjoint, int it, bool snap_u_next, int snap_u_slot, bool snap_v,
+                int snap_v_slot, cudaStream_t st);
+int launch_interaction(const fwi_batch *b, int isae, cudaStream_t st);
+int launch_misfit(const float *data, const float *syn, float *adstf, double *misfit, double *partial, int nshots,
+                  int nrec, int nt, double dt, cudaStream_t st);
+long long misfit_partials(int nrec, int nt);
+int launch_smooth(const double *in, int in_pitch, float *out, int out_pitch, double *tmp, int nx, int nz, int sigma,
+                  cudaStream_t st);
+int launch_vps2lm(float *lam, float *mu, const float *rho, long long n, cudaStream_t st);
+int launch_lm2vps(float *vp, float *vs, const float *rho, long long n, cudaStream_t st);
+int launch_bound(float *bound, int nx, int nz, int pitch, int width, double alpha, int l, int r, int b, int t,
+                 cudaStream_t st);
+int launch_ricker(const double *par, int nsrc, int nt, double dt, float *sx, float *sy, float *sz, cudaStream_t st);
+int launch_prepare(const float *rho, const float *jr, const float *muc, const float *nuc, double dt, long long n,
+                   float *buo, float *buo_j, float *mnc, cudaStream_t st);
+int tile_count();
+
+static bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+
+#define REQUIRE(cond, ...)                                        \
+    do {                                                          \
+        if (!(cond)) return set_error(FWI_EINVAL, __VA_ARGS__);   \
+    } while (0)
+
+static int check_batch(const fwi_batch *b, int adjoint, int it0, int nsteps) {
+    REQUIRE(b, "batch is NULL");
+    REQUIRE(b->mode == FWI_SH || b->mode == FWI_PSV || b->mode == FWI_SPIN, "mode %d unknown", b->mode);
+    REQUIRE(b->nx >= 1 && b->nz >= 1, "grid %dx%d is empty", b->nx, b->nz);
+    REQUIRE(b->pitch >= b->nz && b->pitch % 4 == 0, "pitch %d must be >= nz (%d) and a multiple of 4", b->pitch,
+            b->nz);
+    REQUIRE(b->nshots >= 1 && b->nshots <= 65535, "nshots %d out of range [1, 65535]", b->nshots);
+    REQUIRE((long long)b->nx * b->nz < (1ll << 31), "grid of %lld cells exceeds 2^31", (long long)b->nx * b->nz);
+    REQUIRE(b->cur == 0 || b->cur == 1, "cur must be 0 or 1");
+    REQUIRE(b->tile >= 0 && b->tile < tile_count(), "tile variant %d unknown", b->tile);
+    REQUIRE(b->nt >= 1, "nt must be >= 1");
+    REQUIRE(it0 >= 0 && nsteps >= 0 && (long long)it0 + nsteps <= b->nt, "steps [%d, %d) outside [0, nt=%d)", it0,
+            it0 + nsteps, b->nt);
+    REQUIRE(b->dx > 0.f && b->dz > 0.f && b->dt > 0.0, "dx, dz and dt must be positive");
+    const int ns = b->mode == FWI_SH ? 2 : b->mode == FWI_PSV ? 3 : 6;
+    const int nv = b->mode == FWI_SH ? 1 : b->mode == FWI_PSV ? 2 : 3;
+    for (int h = 0; h < 2; h++) {
+        for (int f = 0; f < ns; f++)
+            REQUIRE(b->sig[h][f] && aligned16(b->sig[h][f]), "sig[%d][%d] NULL or not 16-byte aligned", h, f);
+        for (int q = 0; q < nv; q++)
+            REQUIRE(b->vel[h][q] && aligned16(b->vel[h][q]), "vel[%d][%d] NULL or not 16-byte aligned", h, q);
+    }
+    for (int q = 0; q < nv; q++) REQUIRE(b->disp[q] && aligned16(b->disp[q]), "disp[%d] NULL or misaligned", q);
+    REQUIRE(b->buo && b->bound && b->mu && aligned16(b->buo) && aligned16(b->bound) && aligned16(b->mu),
+            "buo, bound and mu must be non-NULL and 16-byte aligned");
+    if (b->mode != FWI_SH) REQUIRE(b->lam && aligned16(b->lam), "lam must be non-NULL and 16-byte aligned");
+    if (b->mode == FWI_SPIN)
+        REQUIRE(b->buo_j && b->nu && b->mnc && aligned16(b->buo_j) && aligned16(b->nu) && aligned16(b->mnc),
+                "spin needs buo_j, nu and mnc (16-byte aligned)");
+    if (b->inj_ptr) {
+        REQUIRE(b->inj_cell && b->inj_row, "inj_cell and inj_row are required with inj_ptr");
+        if (b->mode == FWI_SH) REQUIRE(b->stf[1], "SH injection needs stf[1]");
+        else REQUIRE(b->stf[0] && b->stf[2], "P-SV injection needs stf[0] and stf[2]");
+    }
+    if (b->nrec > 0 && !adjoint) REQUIRE(b->rec_cell, "rec_cell is required when nrec > 0");
+    if (adjoint) {
+        REQUIRE(b->sae >= 1, "the adjoint needs adjoint_interval >= 1");
+        REQUIRE(b->nsa >= 1, "the adjoint needs nsa >= 1 snapshots");
+        if (b->mode == FWI_SH) REQUIRE(b->snap_u[1], "SH adjoint needs snap_u[1]");
+        else REQUIRE(b->snap_u[0] && b->snap_u[2], "P-SV adjoint needs snap_u[0] and snap_u[2]");
+        REQUIRE(b->mode != FWI_SPIN, "the spin adjoint is not provided");
+        // the correlation at step it reads slot it/sae (solver.py:315-318)
+        const int last = it0 + nsteps - 1;
+        if (nsteps > 0) {
+            const int last_corr = last - last % b->sae;
+            REQUIRE(last_corr < it0 || last_corr / b->sae < b->nsa,
+                    "adjoint step %d needs snapshot %d but only %d exist (nt must not exceed nsa*sae)", last_corr,
+                    last_corr / b->sae, b->nsa);
+        }
+    }
+    return 0;
+}
+
+}  // namespace fwi
+
+using namespace fwi;
+
+extern "C" {
+
+int fwi_abi_version(void) { return FWI_ABI_VERSION; }
+
+int fwi_last_error(char *buf, size_t len) {
+    if (buf && len) {
+        strncpy(buf, g_msg, len - 1);
+        buf[len - 1] = '\0';
+    }
+    return g_code;
+}
+
+int fwi_vps2lm(float *lam_io, float *mu_io, const float *rho, long long n, void *stream) {
+    REQUIRE(lam_io && mu_io && rho && n >= 0, "fwi_vps2lm: NULL pointer or negative size");
+    if (n == 0) return 0;
+    return launch_vps2lm(lam_io, mu_io, rho, n, (cudaStream_t)stream);
+}
+
+int fwi_lm2vps(float *vp_io, float *vs_io, const float *rho, long long n, void *stream) {
+    REQUIRE(vp_io && vs_io && rho && n >= 0, "fwi_lm2vps: NULL pointer or negative size");
+    if (n == 0) return 0;
+    return launch_lm2vps(vp_io, vs_io, rho, n, (cudaStream_t)stream);
+}
+
+int fwi_set_bound(float *bound, int nx, int nz, int pitch, int width, double alpha, int left, int right, int bottom,
+                  int top, void *stream) {
+    REQUIRE(bound && nx >= 1 && nz >= 1 && pitch >= nz, "fwi_set_bound: bad arguments");
+    return launch_bound(bound, nx, nz, pitch, width, alpha, left, right, bottom, top, (cudaStream_t)stream);
+}
+
+int fwi_ricker(const double *params, int nsrc, int nt, double dt, float *stf_x, float *stf_y, float *stf_z,
+               void *stream) {
+    REQUIRE(params && nsrc >= 0 && nt >= 0 && nsrc <= 65535, "fwi_ricker: bad arguments");
+    if (nsrc == 0 || nt == 0) return 0;
+    return launch_ricker(params, nsrc, nt, dt, stf_x, stf_y, stf_z, (cudaStream_t)stream);
+}
+
+int fwi_prepare_model(const float *rho, const float *j, const float *mu_c, const float *nu_c, double dt, long long n,
+                      float *buo, float *buo_j, float *mnc, void *stream) {
+    REQUIRE(rho && buo && n >= 0, "fwi_prepare_model: rho and buo are required");
+    REQUIRE(!buo_j || j, "fwi_prepare_model: buo_j needs j");
+    REQUIRE(!mnc || (mu_c && nu_c), "fwi_prepare_model: mnc needs mu_c and nu_c");
+    if (n == 0) return 0;
+    return launch_prepare(rho, j, mu_c, nu_c, dt, n, buo, buo_j, mnc, (cudaStream_t)stream);
+}
+
+int fwi_run(fwi_batch *b, int adjoint, int it0, int nsteps, void *stream) {
+    int rc = check_batch(b, adjoint, it0, nsteps);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long field = (long long)b->nshots * b->nx * b->pitch;
+    const int sae = b->sae, nsa = b->nsa;
+    if (!adjoint && sae > 0 && nsteps > 0 && (it0 + 1) % sae == 0) {
+        // snapshot of the state before step it0 (solver.py:194-203)
+        const int slot = nsa - (it0 + 1) / sae;
+        if (slot >= 0 && slot < nsa) {
+            for (int c = 0; c < 3; c++) {
+                const int q = b->mode == FWI_SH ? (c == 1 ? 0 : -1) : (c == 0 ? 0 : c == 2 ? 1 : 2);
+                if (q < 0 || !b->snap_u[c] || (b->mode == FWI_PSV && c == 1)) continue;
+                cudaError_t e = cudaMemcpyAsync(b->snap_u[c] + slot * field, b->disp[q], field * sizeof(float),
+                                                cudaMemcpyDeviceToDevice, st);
+                if (e != cudaSuccess) return set_error(FWI_ECUDA, "snapshot copy: %s", cudaGetErrorString(e));
+            }
+        }
+    }
+    for (int it = it0; it < it0 + nsteps; it++) {
+        bool su = false, sv = false;
+        int sus = 0, svs = 0;
+        if (!adjoint && sae > 0) {
+            if (it + 1 < it0 + nsteps && (it + 2) % sae == 0) {
+                sus = nsa - (it + 2) / sae;
+                su = sus >= 0 && sus < nsa;
+            }
+            if ((it + 1) % sae == 0) {
+                svs = nsa - (it + 1) / sae;
+                sv = svs >= 0 && svs < nsa;
+            }
+        }
+        rc = launch_step(b, adjoint, it, su, sus, sv, svs, st);
+        if (rc) return rc;
+        b->cur ^= 1;
+        if (adjoint && it % sae == 0) {
+            rc = launch_interaction(b, it / sae, st);
+            if (rc) return rc;
+        }
+    }
+    return 0;
+}
+
+long long fwi_misfit_partials(int nrec, int nt) { return misfit_partials(nrec, nt); }
+
+int fwi_misfit(const float *data, const float *syn, float *adstf, double *misfit, double *partial, int nshots,
+               int nrec, int nt, double dt, void *stream) {
+    REQUIRE(data && syn && adstf && misfit && partial, "fwi_misfit: NULL pointer");
+    REQUIRE(nshots >= 1 && nshots <= 65535 && nrec >= 0 && nrec <= 65535 && nt >= 0,
+            "fwi_misfit: nshots in [1, 65535], nrec in [0, 65535], nt >= 0");
+    if (nrec == 0 || nt == 0) {
+        cudaError_t e = cudaMemsetAsync(misfit, 0, sizeof(double) * nshots, (cudaStream_t)stream);
+        return e == cudaSuccess ? 0 : set_error(FWI_ECUDA, "fwi_misfit: %s", cudaGetErrorString(e));
+    }
+    return launch_misfit(data, syn, adstf, misfit, partial, nshots, nrec, nt, dt, (cudaStream_t)stream);
+}
+
+int fwi_smooth(const double *in, int in_pitch, float *out, int out_pitch, double *tmp, int nx, int nz, int sigma,
+               void *stream) {
+    REQUIRE(in && out && tmp, "fwi_smooth: NULL pointer");
+    REQUIRE(nx >= 1 && nz >= 1 && in_pitch >= nz && out_pitch >= nz, "fwi_smooth: bad grid or pitch");
+    REQUIRE(sigma >= 1, "fwi_smooth: sigma must be >= 1 (the reference divides by sigma)");
+    REQUIRE(6ll * sigma < (1 << 20), "fwi_smooth: sigma too large");
+    return launch_smooth(in, in_pitch, out, out_pitch, tmp, nx, nz, sigma, (cudaStream_t)stream);
+}
+
+}  // extern "C"
