@@ -1,0 +1,449 @@
+#!/usr/bin/env python
+"""Benchmark of the FWI hot path: batched P-SV forward + adjoint gradient.
+
+Workload (the P-SV gradient configuration): 512 x 512 grid, h = 10 m,
+vp 3000 / vs 1732 (+-5 % checkerboard in 32 x 32-cell squares for the true
+model, homogeneous start) / rho 2600, 32 Ricker sources (f0 = 8 Hz) evenly
+spaced at z = 10 cells, 256 receivers at z = 12 cells, dt = 1e-3 s,
+nt = 4000, 20-cell sponge on the left, right and bottom, adjoint interval 10,
+smoothing sigma 4.  Observed data come from the checkerboard model (computed
+once, untimed).  One step = one gradient of all 32 shots: batched forward with
+snapshots, misfit and adjoint source, batched adjoint with the k_lam/k_mu
+interaction, Gaussian smoothing.  Cell-updates per step =
+32 * 512 * 512 * 4000 * 2 (forward and adjoint counted separately).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line (rank 0).  ``value`` is measured with every input in HBM;
+``e2e`` through the plugin API (seispie_b200.solver.b200.compute_gradient)
+with the observed traces in host memory, their upload and the gradient's
+download inside the timed region.  ``--impl reference`` times the CPU
+restatement of the reference's arithmetic (oracle/, float32, all host threads)
+on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import contextlib
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Gcell-updates/s (P-SV forward+adjoint gradient, batched shots)"
+UNIT = "Gcell-updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--nx", type=int, default=512)
+    ap.add_argument("--nz", type=int, default=512)
+    ap.add_argument("--nt", type=int, default=4000)
+    ap.add_argument("--shots", type=int, default=32)
+    ap.add_argument("--nrec", type=int, default=256)
+    ap.add_argument("--sae", type=int, default=10)
+    ap.add_argument("--sigma", type=int, default=4)
+    ap.add_argument("--tile", type=int, default=0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="only run a few forward steps (for ncu captures of the step kernel)")
+    ap.add_argument("--autotune", action="store_true", help="time every tile variant and report the best")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ workload
+
+def workload(a):
+    nx, nz, h = a.nx, a.nz, 10.0
+    i, j = np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij")
+    sign = np.where(((i // 32) + (j // 32)) % 2 == 0, 1.0, -1.0)
+    vs_true = (1732.0 * (1 + 0.05 * sign)).ravel().astype(np.float32)
+    n = nx * nz
+    vp = np.full(n, 3000.0, np.float32)
+    rho = np.full(n, 2600.0, np.float32)
+    vs_init = np.full(n, 1732.0, np.float32)
+    f0 = 8.0
+    src = np.array([[(s + 0.5) * nx / a.shots * h, 10 * h, 0, f0, 1.2 / f0, 0.0, 1e10] for s in range(a.shots)])
+    rec = np.array([[(r + 0.5) * nx / a.nrec * h, 12 * h] for r in range(a.nrec)])
+    return dict(nx=nx, nz=nz, h=h, dt=1e-3, vp=vp, rho=rho, vs_true=vs_true, vs_init=vs_init, src=src, rec=rec,
+                absorb=(20, 0.015, 1, 1, 1, 0))
+
+
+def config_of(a, w, extra=None):
+    c = {"workload": "psv_gradient_%dx%d_shots%d_rec%d_nt%d" % (a.nx, a.nz, a.shots, a.nrec, a.nt),
+         "grid": [a.nx, a.nz], "shots": a.shots, "receivers": a.nrec, "nt": a.nt, "adjoint_interval": a.sae,
+         "smooth_sigma": a.sigma, "cells_per_step": 2 * a.shots * a.nx * a.nz * a.nt,
+         "l2": "inputs larger than L2 (wavefields of all shots and the snapshots exceed 126 MB); no flush",
+         "parallelism": "shots"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ---------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+        return False
+
+    def summary(self):
+        if self.proc is None:
+            return None
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        for r in rows:
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"),
+                               r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ------------------------------------------------------------ reference arm
+
+def cpu_sample(a, w, seconds):
+    """Time the oracle's float32 restatement of the reference (forward and
+    adjoint of one shot, all host threads) for about ``seconds``; returns
+    (cell-updates/s, sample description, threads)."""
+    from oracle.oracle import Oracle, point_ids, source_time_functions
+    o = Oracle("f32")
+    nx, nz, h, dt = w["nx"], w["nz"], w["h"], w["dt"]
+    lam, mu = o.vps2lm(w["vp"], w["vs_init"], w["rho"])
+    bound = o.set_bound(nx, nz, *w["absorb"])
+    p = dict(rho=w["rho"], lam=lam, mu=mu, bound=bound)
+    sid = point_ids(w["src"], np.float32(h), np.float32(h), nz)
+    rid = point_ids(w["rec"], np.float32(h), np.float32(h), nz)
+    # calibrate on a short run, then size the sample to ~seconds
+    nt0 = 20
+    stf = source_time_functions(w["src"][:1], nt0, dt)
+    t = time.perf_counter()
+    o.forward("psv", nx, nz, h, h, dt, nt0, p, sid[:1], stf, 0, rid)
+    rate0 = nx * nz * nt0 / (time.perf_counter() - t)
+    nt = int(max(2 * a.sae, min(a.nt, seconds * rate0 / 2 / nx / nz)))
+    nt -= nt % a.sae
+    stf = source_time_functions(w["src"][:1], nt, dt)
+    t = time.perf_counter()
+    obs, _, sn = o.forward("psv", nx, nz, h, h, dt, nt, p, sid[:1], stf, 0, rid, sae=a.sae, nsa=nt // a.sae,
+                           snapshots=True)
+    ad = np.random.default_rng(0).standard_normal(len(rid) * nt).astype(np.float32)
+    k = [np.zeros(nx * nz, np.float32) for _ in range(3)]
+    o.adjoint_psv(nx, nz, h, h, dt, nt, p, rid, ad, ad, a.sae, sn, k[0], k[1], k[2])
+    el = time.perf_counter() - t
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    sample = "1 shot of %dx%d, nt=%d forward+adjoint (oracle float32 restatement of the reference)" % (nx, nz, nt)
+    return 2 * nx * nz * nt / el / 1e9, sample, threads
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w = workload(a)
+    vals = []
+    sample = threads = None
+    for s in range(a.warmup + a.steps):
+        v, sample, threads = cpu_sample(a, w, a.cpu_seconds / max(1, a.steps))
+        if s >= a.warmup:
+            vals.append(v)
+    v = statistics.median(vals)
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": 2 * a.shots * a.nx * a.nz * a.nt / (v * 1e9) * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": config_of(a, w),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------- GPU arm
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference(a)
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    from seispie_b200 import _lib, engine
+    from seispie_b200.engine import Grid, ShotBatch, adjoint_injection_lists, build_model, injection_lists
+
+    lib = _lib.load()
+    w = workload(a)
+    nx, nz, h, dt, nt = w["nx"], w["nz"], w["h"], w["dt"], a.nt
+    sid = engine.point_ids(w["src"], np.float32(h), np.float32(h), nz)
+    rid = engine.point_ids(w["rec"], np.float32(h), np.float32(h), nz)
+    grid = Grid(nx, nz, float(np.float32(h)), float(np.float32(h)))
+    m_true = build_model("psv", grid, dt, dict(vp=w["vp"], vs=w["vs_true"], rho=w["rho"]), w["absorb"], dev)
+    m_init = build_model("psv", grid, dt, dict(vp=w["vp"], vs=w["vs_init"], rho=w["rho"]), w["absorb"], dev)
+    stf, _ = engine.ricker_stf(w["src"], nt, dt, dev)
+    nshots = a.shots
+    inj = injection_lists(nshots, sid, lambda s: s)
+
+    if a.profile_case:
+        b = ShotBatch(m_init, nshots, nt, rid, tile=a.tile)
+        d = b.desc(inj=inj, stf=stf)
+        b.clear()
+        b.run(d, False, 0, min(nt, 20))
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_case": True, "steps": min(nt, 20)}))
+        return
+
+    # observed data from the checkerboard model (untimed)
+    bt = ShotBatch(m_true, nshots, nt, rid, tile=a.tile)
+    bt.clear()
+    bt.run(bt.desc(inj=inj, stf=stf), False, 0, nt)
+    data = [bt.obs[0].clone(), None, bt.obs[2].clone()]
+    del bt
+
+    nsa = nt // a.sae
+    b = ShotBatch(m_init, nshots, nt, rid, sae=a.sae, nsa=nsa, snapshots=True, tile=a.tile)
+    k_lam = torch.zeros((nx, m_init.grid.pitch), dtype=torch.float64, device=dev)
+    k_mu = torch.zeros_like(k_lam)
+    adstf = [torch.empty(nshots * a.nrec * nt, dtype=torch.float32, device=dev) if c != 1 else None
+             for c in range(3)]
+    fwd = b.desc(inj=inj, stf=stf)
+    adj = b.desc(inj=adjoint_injection_lists(nshots, rid), stf=adstf, record=False, kernels=(k_lam, k_mu, None))
+    stream = torch.cuda.current_stream()
+
+    ev = {}
+
+    def gradient(record=False):
+        k_lam.zero_()
+        k_mu.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e2 = torch.cuda.Event(enable_timing=True)
+        e3 = torch.cuda.Event(enable_timing=True)
+        b.clear()
+        e0.record(stream)
+        b.run(fwd, False, 0, nt)
+        e1.record(stream)
+        mis = [engine.misfit(data[c], b.obs[c], adstf[c], nshots, a.nrec, nt, dt) for c in (0, 2)]
+        b.clear()
+        e2.record(stream)
+        b.run(adj, True, 0, nt)
+        e3.record(stream)
+        g = engine.smooth(k_mu, m_init.grid, a.sigma)
+        if world > 1:
+            dist.all_reduce(k_mu)
+        if record:
+            ev.setdefault("fwd", []).append((e0, e1))
+            ev.setdefault("adj", []).append((e2, e3))
+        return mis, g
+
+    def tune():
+        best = None
+        for t in _lib.tile_variants():
+            bb = ShotBatch(m_init, nshots, nt, rid, tile=t)
+            dd = bb.desc(inj=inj, stf=stf)
+            bb.clear()
+            bb.run(dd, False, 0, 20)
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record()
+            bb.run(dd, False, 20, 100)
+            s1.record()
+            torch.cuda.synchronize()
+            ms = s0.elapsed_time(s1) / 100
+            if best is None or ms < best[1]:
+                best = (t, ms)
+            del bb
+        return best
+
+    tuned = None
+    if a.autotune:
+        tuned = tune()
+        b.tile = fwd.tile = adj.tile = tuned[0]
+
+    for _ in range(a.warmup):
+        gradient()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches0 = lib.fwi_launch_count()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        t0.record(stream)
+        for _ in range(a.steps):
+            mis, g = gradient(record=True)
+        t1.record(stream)
+        torch.cuda.synchronize()
+    launches = lib.fwi_launch_count() - launches0
+    ms = t0.elapsed_time(t1) / a.steps
+    if world > 1:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+        dist.barrier()
+    cells_rank = 2 * nshots * nx * nz * nt
+    value = cells_rank * world / (ms * 1e-3) / 1e9
+
+    # roofline of the dominant kernel: the fused P-SV step (forward launches)
+    fwd_ms = statistics.median(e0.elapsed_time(e1) for e0, e1 in ev["fwd"])
+    adj_ms = statistics.median(e0.elapsed_time(e1) for e0, e1 in ev["adj"])
+    per_launch_s = fwd_ms * 1e-3 / nt
+    bytes_per_launch = nshots * nx * nz * (72 + 8.0 / a.sae)
+    achieved = bytes_per_launch / per_launch_s / 1e9
+    peak, peak_src = 6650.0, "fallback"
+    try:
+        pk = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peak, peak_src = float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        pass
+    traffic = None
+    try:
+        prof = json.load(open(os.path.join(ROOT, "profiles", "step_kernel_psv_traffic.json")))
+        traffic = prof["dram_bytes_per_launch_full_workload"]
+    except Exception:
+        pass
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "peak_source": peak_src, "kernel": "step_kernel<P-SV> (forward launches)",
+            "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_us": per_launch_s * 1e6,
+            "adjoint_step_us": adj_ms * 1e3 / nt}
+    misfit_total = float(sum(m.sum().item() for m in mis))
+    del b, fwd, adj
+    torch.cuda.empty_cache()
+
+    # ----------------------------------------------------------------- e2e
+    e2e = None
+    if not a.no_e2e:
+        e2e = run_e2e(a, w, dev, world, rank, data)
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        v, sample, threads = cpu_sample(a, w, a.cpu_seconds)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        extra = {"tile": _lib.tile_shape(b_tile(a, tuned)), "misfit": misfit_total}
+        if tuned:
+            extra["autotune_ms_per_fwd_step"] = tuned[1]
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config_of(a, w, extra),
+                "clocks": clk.summary(), "gpu_launches": launches, "roofline": roof, "e2e": e2e,
+                "cpu_baseline": cpu, "impl": "b200"}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def b_tile(a, tuned):
+    return tuned[0] if tuned else a.tile
+
+
+def run_e2e(a, w, dev, world, rank, data):
+    """compute_gradient() of the b200 plugin with host-resident traces."""
+    import torch
+    from seispie_b200.solver import b200
+
+    td = tempfile.mkdtemp()
+    nx, nz, h = w["nx"], w["nz"], w["h"]
+    from seispie_b200.io import write_model
+    write_model(td + "/init", nx, nz, h, h, dict(vp=w["vp"], vs=w["vs_init"], rho=w["rho"]))
+    np.savetxt(td + "/src.dat", w["src"])
+    np.savetxt(td + "/rec.dat", w["rec"])
+    os.makedirs(td + "/out", exist_ok=True)
+    s = b200()
+    s.config = dict(nt=str(a.nt), dt=str(w["dt"]), sh="no", psv="yes", spin="no", abs_left="yes", abs_right="yes",
+                    abs_top="no", abs_bottom="yes", abs_width="20", abs_alpha="0.015", save_coordinates="",
+                    combine_sources="no", save_snapshot="0", adjoint_interval=str(a.sae), smooth=str(a.sigma),
+                    tile=str(a.tile))
+    s.path = dict(model_init=td + "/init", model_true=td + "/init", sources=td + "/src.dat",
+                  stations=td + "/rec.dat", output=td + "/out")
+    s.mpi = None
+    with contextlib.redirect_stdout(io.StringIO()):
+        s.setup(None)
+        s.import_model(0)
+        s.import_sources()
+        s.import_stations()
+    dx = data[0].view(a.shots, a.nrec * a.nt).cpu().numpy()
+    dz = data[2].view(a.shots, a.nrec * a.nt).cpu().numpy()
+    s.syn_x = [np.ascontiguousarray(dx[i]) for i in range(a.shots)]
+    s.syn_z = [np.ascontiguousarray(dz[i]) for i in range(a.shots)]
+    s.syn_y = []
+    h2d = sum(x.nbytes for x in s.syn_x + s.syn_z)
+    d2h = 2 * nx * nz * 4  # gradient and model returned as float32
+    with contextlib.redirect_stdout(io.StringIO()):
+        for _ in range(max(1, a.warmup)):
+            s.compute_gradient()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for _ in range(a.steps):
+            s.compute_gradient()
+        torch.cuda.synchronize()
+        el = (time.perf_counter() - t) / a.steps
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([el], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        el = float(tt.item())
+    cells = 2 * a.shots * nx * nz * a.nt * world
+    return {"value": cells / el / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "ms_per_step": el * 1e3, "api": "seispie_b200.solver.b200.compute_gradient"}
+
+
+if __name__ == "__main__":
+    main()

@@ -104,9 +104,19 @@ typedef struct fwi_batch {
 /* ABI version of the loaded library (FWI_ABI_VERSION). */
 int fwi_abi_version(void);
 
+/* Number of kernels this library has launched in the process so far (for
+ * launch accounting by benchmarks).  No counterpart in the reference. */
+long long fwi_launch_count(void);
+
 /* Copy the last error message of the calling thread into buf (always NUL
  * terminated); returns the status code of that error (0 if none). */
 int fwi_last_error(char *buf, size_t len);
+
+/* Interior tile (x rows, z columns) of step-kernel variant `tile`
+ * (fwi_batch.tile); returns FWI_EINVAL for an unknown variant.  Variant 0
+ * is the library default.  No counterpart in the reference (its kernels use
+ * a 1-D grid of threads_per_block threads, fd2d.py:184-187). */
+int fwi_tile_shape(int tile, int *tx, int *tz);
 
 /* vp/vs -> lambda/mu in place: lam_io holds vp and mu_io holds vs on entry.
  * Replaces vps2lm, seispie/solver/fd2d/fd2d.py:21-33 (launched at

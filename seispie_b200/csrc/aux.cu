@@ -282,6 +282,7 @@ int launch_smooth(const double *in, int in_pitch, float *out, int out_pitch, dou
                   cudaStream_t st) {
     const int R = min((int)ceil(6.0 * sigma), max(nx, nz));
     const size_t sm = sizeof(double) * (R + 1);
+    if (sm > 48 * 1024) return set_error(FWI_ERANGE, "fwi_smooth: truncation radius %d exceeds 6143 taps", R);
     dim3 grid((nz + 127) / 128, nx);
     smooth_x_kernel<<<grid, 128, sm, st>>>(in, in_pitch, tmp, nx, nz, R, (double)sigma);
     int rc = check_launch("smooth_x");

@@ -3,6 +3,7 @@
 // time loop that enqueues the fused step kernels.
 #include <cstdarg>
 #include <cstdio>
+#include <atomic>
 #include <cstring>
 
 #include "common.cuh"
@@ -21,7 +22,10 @@ int set_error(int code, const char *fmt, ...) {
     return code;
 }
 
+static std::atomic<long long> g_launches{0};
+
 int check_launch(const char *what) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_error(FWI_ECUDA, "%s: %s", what, cudaGetErrorString(e));
     return 0;
@@ -44,6 +48,7 @@ int launch_ricker(const double *par, int nsrc, int nt, double dt, float *sx, flo
 int launch_prepare(const float *rho, const float *jr, const float *muc, const float *nuc, double dt, long long n,
                    float *buo, float *buo_j, float *mnc, cudaStream_t st);
 int tile_count();
+bool tile_shape(int tile, int *tx, int *tz);
 
 static bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
 
@@ -113,12 +118,22 @@ extern "C" {
 
 int fwi_abi_version(void) { return FWI_ABI_VERSION; }
 
+long long fwi_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
 int fwi_last_error(char *buf, size_t len) {
     if (buf && len) {
         strncpy(buf, g_msg, len - 1);
         buf[len - 1] = '\0';
     }
     return g_code;
+}
+
+int fwi_tile_shape(int tile, int *tx, int *tz) {
+    int x = 0, z = 0;
+    REQUIRE(tile_shape(tile, &x, &z), "tile variant %d unknown", tile);
+    if (tx) *tx = x;
+    if (tz) *tz = z;
+    return 0;
 }
 
 int fwi_vps2lm(float *lam_io, float *mu_io, const float *rho, long long n, void *stream) {

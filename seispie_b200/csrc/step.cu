@@ -14,7 +14,7 @@
 //
 // Design.  A CTA owns a TX x TZ interior tile of one shot.  It stages in
 // shared memory (cp.async, 16-byte chunks, zero-filled outside the grid):
-//   stress  rows x0-3 .. x0+TX+1, columns z0-4 .. z0+TZ+3
+//   stress  rows x0-3 .. x0+TX+2, columns z0-4 .. z0+TZ+3
 //   velocity, dt/rho, sponge   rows x0-1 .. x0+TX+1, same columns
 //   displacement and stiffness of the interior
 // computes the new velocity on the interior plus the one-left / two-right
@@ -74,7 +74,9 @@ struct StepArgs {
 template <int MODE, int TX, int TZ>
 struct Tile {
     using F = Fields<MODE>;
-    static constexpr int SX = TX + 5, SZ = TZ + 8;  // stress region
+    // stress region: rows x0-3 .. x0+TX+2 (D- of the velocity halo row
+    // x0+TX+1 reaches x0+TX+2), columns z0-4 .. z0+TZ+3
+    static constexpr int SX = TX + 6, SZ = TZ + 8;
     static constexpr int VX = TX + 3, RVZ = TZ + 3;  // velocity rows / computed columns
     static constexpr int S_SZ = F::NS * SX * SZ;
     static constexpr int V_SZ = F::NV * VX * SZ;
@@ -368,6 +370,13 @@ static int launch_mode(const StepArgs &a, int nshots, int tile, cudaStream_t st)
 }
 
 int tile_count() { return kNumTiles; }
+
+bool tile_shape(int tile, int *tx, int *tz) {
+    if (tile < 0 || tile >= kNumTiles) return false;
+    *tx = kTiles[tile].tx;
+    *tz = kTiles[tile].tz;
+    return true;
+}
 
 size_t step_smem_bytes(int mode, int tile) {
     if (tile < 0 || tile >= kNumTiles) return 0;

@@ -1,0 +1,476 @@
+"""The ``b200`` solver plugin: a drop-in for seispie's ``fd2d`` solver.
+
+sprun loads a solver as ``getattr(import_module('seispie.solver.' + method),
+method)()`` and then sets ``.config`` (a section of strings), ``.path`` (a
+dict of absolute paths) and ``.mpi`` before calling ``setup(workflow)``
+(scripts/sprun:79-86).  This class keeps that contract and the public method
+set and attributes of ``seispie.solver.fd2d.fd2d`` (fd2d.py:110-443):
+
+  setup, import_model, import_sources, import_stations, import_traces,
+  run_forward, run_adjoint, run_kernel, compute_misfit, compute_gradient,
+  update_model, smooth, export_field, setup_adjoint, clear_kernels,
+  clear_wavefields; attributes nx, nz, dx, dz, npt, nt, dt, nsrc, nrec,
+  stream (has .synchronize()) and mu (has .copy_to_host(out, stream)).
+
+Differences that a caller can see, all deliberate:
+  * All shots of run_kernel are stepped together in one batched launch per
+    time step (the reference loops over shots one after another).
+  * The P-SV adjoint works (the reference's raises NameError,
+    solver.py:324-329) and also yields k_lam and k_rho.
+  * Sensitivity kernels accumulate in FP64; the misfit is summed in FP64.
+  * Without a GPU the solver refuses to start; there is no CPU path.
+"""
+from __future__ import annotations
+
+import os
+from os import makedirs, path
+from time import time
+
+import numpy as np
+import torch
+
+from .. import engine
+from .._lib import FWI_PSV, FWI_SH, FWI_SPIN, MODES
+from ..engine import DeviceModel, Grid, ShotBatch
+
+
+class DeviceArray:
+    """A device field with the numba DeviceNDArray method the upper layers
+    use: ``copy_to_host(ary, stream)`` (optimize/base.py:59-61)."""
+
+    def __init__(self, tensor: torch.Tensor, nz: int | None = None):
+        self.tensor = tensor
+        self.nz = nz
+
+    def _flat(self) -> torch.Tensor:
+        t = self.tensor
+        if t.dim() == 2 and self.nz is not None:
+            t = t[:, : self.nz]
+        return t.reshape(-1)
+
+    @property
+    def size(self) -> int:
+        return self._flat().numel()
+
+    def copy_to_host(self, ary: np.ndarray | None = None, stream=None) -> np.ndarray:
+        with torch.cuda.stream(stream) if isinstance(stream, torch.cuda.Stream) else _nullctx():
+            host = self._flat().to(torch.float32).cpu().numpy()
+        if ary is None:
+            return host
+        ary.reshape(-1)[:] = host
+        return ary
+
+
+def infer_grid(x: np.ndarray, z: np.ndarray, npt):
+    """Grid size and spacing from the coordinate arrays of a model file.
+
+    First the reference's formula (fd2d.py:189-196): nx = rint(sqrt(npt*lx/lz)),
+    dx = lx/(nx-1) as numpy float32.  It is exact for square grids but not in
+    general (1024x512 gives nx = 1025, because lx/lz = (nx-1)/(nz-1), not
+    nx/nz); when its nx*nz differs from npt, nz is read from the layout
+    instead: the cells k = i*nz + j of row i share one x, so nz is the length
+    of the leading run of x == x[0]."""
+    lx = x.max() - x.min()
+    lz = z.max() - z.min()
+    nx = int(np.rint(np.sqrt(npt * lx / lz)))
+    nz = int(np.rint(np.sqrt(npt * lz / lx)))
+    if nx * nz != npt:
+        nz = int(np.argmax(x != x[0])) if np.any(x != x[0]) else int(npt)
+        nx = int(npt) // nz
+        if nx * nz != npt:
+            raise ValueError("model of %d points is not a regular grid" % npt)
+    return nx, nz, lx / (nx - 1), lz / (nz - 1)
+
+
+class _nullctx:
+    def __enter__(self):
+        return None
+
+    def __exit__(self, *a):
+        return False
+
+
+class b200:
+    """B200 FWI solver plugin (drop-in for ``fd2d``)."""
+
+    # ------------------------------------------------------------------ setup
+    def setup(self, workflow):
+        """fd2d.py:111-120, plus the device and stream of this solver."""
+        if not torch.cuda.is_available():
+            raise RuntimeError("seispie_b200 needs a CUDA device; there is no CPU path")
+        from .. import _lib
+        _lib.load()  # fail here, loudly, if the CUDA library is missing
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        self.stream = torch.cuda.Stream(self.device)
+        self.nt = int(self.config["nt"])
+        self.dt = float(self.config["dt"])
+        self.sh = 1 if self.config["sh"] == "yes" else 0
+        self.psv = 1 if self.config["psv"] == "yes" else 0
+        self.spin = 1 if self.config.get("spin", "no") == "yes" else 0
+        self.sae = 0
+        self.nsa = 0
+        self.tile = int(self.config.get("tile", 0))
+        self.batch_memory = float(self.config.get("batch_memory_gb", 0)) * 2 ** 30
+        self.kernel_rho = self.config.get("kernel_rho", "no") == "yes"
+        self.model = None
+
+    def _ctx(self):
+        return torch.cuda.stream(self.stream)
+
+    @property
+    def modes(self):
+        """Wave types this configuration runs, in the reference's order."""
+        m = []
+        if self.sh:
+            m.append(FWI_SH)
+        if self.psv:
+            m.append(FWI_SPIN if self.spin else FWI_PSV)
+        return m
+
+    # -------------------------------------------------------------- sources
+    def import_sources(self):
+        """fd2d.py:122-146: src_id by round-half-even of x/dx and z/dz; the
+        Ricker time functions are evaluated on the device (fwi_ricker)."""
+        src = np.loadtxt(self.path["sources"], ndmin=2)
+        self.nsrc = src.shape[0]
+        self.src = src
+        self.src_id = self._point_ids(src)
+        with self._ctx():
+            (self.stf_x, self.stf_y, self.stf_z), self._stf_par = engine.ricker_stf(src, self.nt, self.dt,
+                                                                                   self.device, self.stream)
+
+    def import_stations(self):
+        """fd2d.py:148-165."""
+        rec = np.loadtxt(self.path["stations"], ndmin=2)
+        self.nrec = rec.shape[0]
+        self.rec = rec
+        self.rec_id = self._point_ids(rec)
+
+    def _point_ids(self, pts: np.ndarray) -> np.ndarray:
+        ids = engine.point_ids(pts, self.dx, self.dz, self.nz)
+        if len(ids) and (ids.min() < 0 or ids.max() >= self.nx * self.nz):
+            raise ValueError("a source or station lies outside the %dx%d grid" % (self.nx, self.nz))
+        return ids
+
+    # ---------------------------------------------------------------- model
+    def import_model(self, model_true):
+        """fd2d.py:167-252: read proc000000_<name>.bin, infer the grid, set
+        lambda/mu (vps2lm) and the sponge (set_bound) on the device."""
+        model = dict()
+        model_dir = self.path["model_true"] if model_true else self.path["model_init"]
+        names = (["x", "z", "lambda", "mu", "nu", "j", "lambda_c", "mu_c", "nu_c", "rho"] if self.spin
+                 else ["x", "z", "vp", "vs", "rho"])
+        for name in names:
+            filename = path.join(model_dir, "proc000000_" + name + ".bin")
+            with open(filename, "rb") as f:
+                if not hasattr(self, "npt"):
+                    f.seek(0)
+                    self.npt = np.fromfile(f, dtype="int32", count=1)
+                f.seek(4)
+                model[name] = np.fromfile(f, dtype="float32")
+        x, z = model["x"], model["z"]
+        nx, nz, self.dx, self.dz = infer_grid(x, z, self.npt[0])
+        self.nx, self.nz = nx, nz
+        self.grid = Grid(nx, nz, float(self.dx), float(self.dz))
+        mode = FWI_SPIN if self.spin else (FWI_PSV if self.psv else FWI_SH)
+        with self._ctx():
+            m = DeviceModel(self.grid, mode, self.dt, self.device, self.stream)
+            m.set("rho", model["rho"])
+            lib = engine._lib.load()
+            if self.spin:
+                for dst, src in (("lam", "lambda"), ("mu", "mu"), ("nu", "nu"), ("j", "j"), ("mu_c", "mu_c"),
+                                 ("nu_c", "nu_c")):
+                    m.set(dst, model[src])
+            else:
+                m.set("lam", model["vp"])
+                m.set("mu", model["vs"])
+                engine.check(lib.fwi_vps2lm(engine.ptr(m.lam), engine.ptr(m.mu), engine.ptr(m.rho),
+                                            m.lam.numel(), engine.stream_handle(self.stream)), "fwi_vps2lm")
+            c = self.config
+            engine.check(lib.fwi_set_bound(engine.ptr(m.bound), nx, nz, self.grid.pitch, int(c["abs_width"]),
+                                           float(c["abs_alpha"]), c["abs_left"] == "yes", c["abs_right"] == "yes",
+                                           c["abs_bottom"] == "yes", c["abs_top"] == "yes",
+                                           engine.stream_handle(self.stream)), "fwi_set_bound")
+            m.prepare()
+        self.model = m
+        self.rho = DeviceArray(m.rho, nz)
+        self.lam = DeviceArray(m.lam, nz)
+        self.mu = DeviceArray(m.mu, nz)
+        self.bound = DeviceArray(m.bound, nz)
+        # fd2d.py:250 tests the raw string, so any non-empty value exports
+        if self.config["save_coordinates"]:
+            self.export_field(x, "x")
+            self.export_field(z, "z")
+
+    def export_field(self, field, name, it=0):
+        """fd2d.py:254-261: [int32 npt][float32 field] to output/procIT_name.bin."""
+        if isinstance(field, DeviceArray):
+            field = field.copy_to_host()
+        elif isinstance(field, torch.Tensor):
+            field = field.detach().float().cpu().numpy()
+        name = "proc%06d_%s" % (it, name)
+        with open(self.path["output"] + "/" + name + ".bin", "wb") as f:
+            self.npt.tofile(f)
+            np.asarray(field, dtype="float32").tofile(f)
+
+    def update_model(self, mu):
+        """fd2d.py:442-443: replace mu (only mu) with a fresh upload."""
+        with self._ctx():
+            self.model.mu.copy_(self.model.pad(np.asarray(mu, dtype="float32")))
+
+    # ------------------------------------------------------------- batching
+    def _isrc(self):
+        if self.config["combine_sources"] == "yes":
+            return -1
+        if not hasattr(self, "taskid"):
+            raise AttributeError("combine_sources = no needs a task id (set taskid or use run_kernel)")
+        return self.taskid
+
+    def _shot_bytes(self, mode, snapshots):
+        g = self.grid
+        field = g.nx * g.pitch * 4
+        ns, nv = engine.NS[mode], engine.NV[mode]
+        b = (2 * ns + 3 * nv) * field + 4 * self.nrec * self.nt * nv * 3
+        if snapshots:
+            b += self.nsa * min(nv, 2) * field * (2 if (mode != FWI_SH and self.kernel_rho) else 1)
+        return b
+
+    def _max_batch(self, mode, snapshots):
+        budget = self.batch_memory
+        if budget <= 0:
+            free, _ = torch.cuda.mem_get_info(self.device)
+            budget = 0.8 * free
+        return max(1, int(budget // self._shot_bytes(mode, snapshots)))
+
+    def _shots(self):
+        """Shots of this process: contiguous shards of range(nsrc) across the
+        ranks of self.mpi (the reference gives rank r shot r)."""
+        if not self.mpi:
+            return list(range(self.nsrc))
+        r, n = self.mpi.rank(), self.mpi.size()
+        lo, hi = self.nsrc * r // n, self.nsrc * (r + 1) // n
+        return list(range(lo, hi))
+
+    def _stf(self, mode):
+        return (self.stf_x, self.stf_y, self.stf_z)
+
+    # -------------------------------------------------------------- forward
+    def clear_wavefields(self):
+        for b in getattr(self, "_fwd_batches", {}).values():
+            b.clear()
+
+    def run_forward(self):
+        """solver.py:166-287 for one shot set (all sources when
+        combine_sources = yes, else source taskid): traces in obs_x/y/z,
+        snapshots every save_snapshot steps and output_traces files."""
+        isrc = self._isrc()
+        sfe = int(self.config["save_snapshot"])
+        self._fwd_batches = {}
+        with self._ctx():
+            for mode in self.modes:
+                b = ShotBatch(self.model, 1, self.nt, self.rec_id, tile=self.tile)
+                inj = engine.injection_lists(1, self.src_id, lambda s: isrc)
+                d = b.desc(inj=inj, stf=self._stf(mode))
+                b.clear()
+                it = 0
+                while it < self.nt:
+                    n = self.nt - it
+                    if sfe:
+                        nxt = (it // sfe + 1) * sfe if it > 0 else sfe  # next export step
+                        n = min(n, nxt - it + 1)
+                    b.run(d, False, it, n)
+                    it += n
+                    last = it - 1
+                    if sfe and last > 0 and last % sfe == 0:
+                        names = {FWI_SH: [("vy", "vy")], FWI_PSV: [("vx", "vx"), ("vz", "vz")],
+                                 FWI_SPIN: [("vx", "vx"), ("vz", "vz"), ("vy_c", "ry")]}[mode]
+                        for f, out in names:
+                            self.export_field(b.field(f)[0].reshape(-1), out, last)
+                self._fwd_batches[mode] = b
+                if mode == FWI_SH:
+                    self.obs_y = DeviceArray(b.obs[1])
+                else:
+                    self.obs_x = DeviceArray(b.obs[0])
+                    self.obs_z = DeviceArray(b.obs[2])
+                    if mode == FWI_SPIN:
+                        self.obs_y = DeviceArray(b.obs[1])
+        if "output_traces" in self.path:
+            tracedir = self.path["output_traces"]
+            i = isrc if isrc >= 0 else 0
+            comps = []
+            if self.sh:
+                comps.append(("uy", self.obs_y))
+            if self.psv:
+                comps += [("ux", self.obs_x), ("uz", self.obs_z)]
+                if self.spin:
+                    comps.append(("ry", self.obs_y))
+            for name, arr in comps:
+                np.save("%s/%s_%06d.npy" % (tracedir, name, i), arr.copy_to_host().reshape([self.nrec, self.nt]))
+        self.stream.synchronize()
+
+    # ---------------------------------------------------------------- traces
+    def import_traces(self):
+        """fd2d.py:354-423: observed traces from raw float32 files
+        (vy/vx/vz_%06d.npy), or generated with the current (true) model for
+        every shot -- here all shots in one batched forward."""
+        shots = self._shots()
+        self.syn_x, self.syn_y, self.syn_z = [], [], []
+        if "traces" in self.path:
+            tracedir = self.path["traces"]
+            for i in shots:
+                if self.sh:
+                    self.syn_y.append(np.fromfile("%s/vy_%06d.npy" % (tracedir, i), dtype="float32"))
+                if self.psv:
+                    self.syn_x.append(np.fromfile("%s/vx_%06d.npy" % (tracedir, i), dtype="float32"))
+                    self.syn_z.append(np.fromfile("%s/vz_%06d.npy" % (tracedir, i), dtype="float32"))
+            return
+        tracedir = self.path["output"] + "/traces"
+        if not self.mpi or self.mpi.rank() == 0:
+            print("Generating traces")
+            if not path.exists(tracedir):
+                makedirs(tracedir)
+        if self.mpi:
+            self.mpi.sync()
+        start = time()
+        for mode in self.modes:
+            for chunk in self._chunks(shots, mode, False):
+                b = self._forward_batch(mode, chunk, snapshots=False)
+                for c, lst, nm in ((1, self.syn_y, "vy"), (0, self.syn_x, "vx"), (2, self.syn_z, "vz")):
+                    if b.obs[c] is None or (c == 1 and mode == FWI_SPIN):
+                        continue
+                    tr = b.traces(c).cpu().numpy()
+                    for q, i in enumerate(chunk):
+                        out = np.ascontiguousarray(tr[q]).reshape(-1)
+                        lst.append(out)
+                        out.tofile("%s/%s_%06d.npy" % (tracedir, nm, i))
+        if not self.mpi:
+            print("Elapsed time: %.2fs" % (time() - start))
+            print("")
+
+    def _chunks(self, shots, mode, snapshots):
+        m = self._max_batch(mode, snapshots)
+        return [shots[q:q + m] for q in range(0, len(shots), m)]
+
+    def _forward_batch(self, mode, chunk, snapshots, snap_velocity=False):
+        combine = self.config["combine_sources"] == "yes"
+        with self._ctx():
+            b = ShotBatch(self.model, len(chunk), self.nt, self.rec_id, sae=self.sae, nsa=self.nsa,
+                          snapshots=snapshots, snap_velocity=snap_velocity, tile=self.tile)
+            inj = engine.injection_lists(len(chunk), self.src_id, lambda s: -1 if combine else chunk[s])
+            d = b.desc(inj=inj, stf=self._stf(mode))
+            b.clear()
+            b.run(d, False, 0, self.nt)
+        return b
+
+    # --------------------------------------------------------------- adjoint
+    def setup_adjoint(self):
+        """fd2d.py:263-301: adjoint interval, snapshot count, kernels and the
+        smoothing width.  Snapshots live in HBM (allocated per batch)."""
+        self.sae = int(self.config["adjoint_interval"])
+        self.nsa = int(self.nt / self.sae)
+        self.sigma = int(self.config["smooth"])
+        g = self.grid
+        with self._ctx():
+            self.k_lam_f64 = torch.zeros((g.nx, g.pitch), dtype=torch.float64, device=self.device)
+            self.k_mu_f64 = torch.zeros((g.nx, g.pitch), dtype=torch.float64, device=self.device)
+            self.k_rho_f64 = torch.zeros((g.nx, g.pitch), dtype=torch.float64, device=self.device)
+
+    def clear_kernels(self):
+        with self._ctx():
+            for k in (self.k_lam_f64, self.k_mu_f64, self.k_rho_f64):
+                k.zero_()
+
+    def run_adjoint(self):
+        """solver.py:290-329 for the batch of the last run_kernel chunk."""
+        raise NotImplementedError("run_adjoint is driven by run_kernel, which batches every shot")
+
+    def run_kernel(self, adj):
+        """solver.py:332-404, all shots of this process batched: forward with
+        snapshots, misfit and adjoint source, adjoint with interaction, then
+        the cross-rank sum and the Gaussian smoothing of k_mu."""
+        if not self.mpi:
+            print("Computing kernels" if adj else "Computing misfit")
+        self.setup_adjoint()
+        self.clear_kernels()
+        shots = self._shots()
+        misfit = 0.0
+        data_of = {FWI_SH: [(1, self.syn_y)], FWI_PSV: [(0, self.syn_x), (2, self.syn_z)],
+                   FWI_SPIN: [(0, self.syn_x), (2, self.syn_z)]}
+        for mode in self.modes:
+            snapv = adj and mode != FWI_SH and self.kernel_rho
+            for chunk in self._chunks(shots, mode, adj):
+                b = self._forward_batch(mode, chunk, snapshots=bool(adj), snap_velocity=snapv)
+                n, nrec, nt = len(chunk), self.nrec, self.nt
+                with self._ctx():
+                    adstf = [None, None, None]
+                    for c, lst in data_of[mode]:
+                        data = torch.from_numpy(np.stack([lst[shots.index(i)] for i in chunk]))
+                        data = data.pin_memory().to(self.device, non_blocking=True)
+                        adstf[c] = torch.empty(n * nrec * nt, dtype=torch.float32, device=self.device)
+                        m = engine.misfit(data, b.obs[c], adstf[c], n, nrec, nt, self.dt)
+                        misfit += float(m.sum().item())
+                    if adj:
+                        if mode == FWI_SPIN:
+                            raise NotImplementedError("the spin adjoint is not provided")
+                        kern = (None, self.k_mu_f64, None) if mode == FWI_SH else \
+                               (self.k_lam_f64, self.k_mu_f64, self.k_rho_f64 if snapv else None)
+                        d = b.desc(inj=engine.adjoint_injection_lists(n, self.rec_id), stf=adstf, record=False,
+                                   kernels=kern)
+                        b.clear()
+                        b.run(d, True, 0, nt)
+                del b
+        if self.mpi:
+            misfit = self._mpi_sum_misfit(misfit)
+            self._mpi_sum_kernels()
+        if adj:
+            with self._ctx():
+                self.k_mu = DeviceArray(engine.smooth(self.k_mu_f64, self.grid, self.sigma))
+                self.k_lam = DeviceArray(self.k_lam_f64, self.nz)
+                self.k_rho = DeviceArray(self.k_rho_f64, self.nz)
+        if not self.mpi:
+            print("  misfit = %.2f" % misfit)
+        if adj:
+            return misfit, self.k_mu, self.mu
+        return misfit
+
+    def _mpi_sum_misfit(self, misfit):
+        out = np.zeros(1, dtype="float64")
+        self.mpi.sum(np.array([misfit], dtype="float64"), out)
+        return float(out[0])
+
+    def _mpi_sum_kernels(self):
+        """Cross-rank sum of the FP64 kernels (replaces the file exchange of
+        solver.py:380-393, which also counted the local kernel twice)."""
+        if hasattr(self.mpi, "allreduce_tensor"):
+            self.stream.synchronize()
+            for k in (self.k_lam_f64, self.k_mu_f64, self.k_rho_f64):
+                self.mpi.allreduce_tensor(k)
+        else:
+            for k in (self.k_lam_f64, self.k_mu_f64, self.k_rho_f64):
+                host = k.cpu().numpy()
+                out = np.zeros_like(host)
+                self.mpi.sum(host, out)
+                k.copy_(torch.from_numpy(out))
+
+    def compute_misfit(self):
+        return self.run_kernel(0)
+
+    def compute_gradient(self):
+        """fd2d.py:428-437: (smoothed k_mu, misfit, mu) as host float32."""
+        misfit, kernel, model = self.run_kernel(1)
+        out_k = kernel.copy_to_host(stream=self.stream)
+        out_m = model.copy_to_host(stream=self.stream)
+        self.stream.synchronize()
+        return out_k, misfit, out_m
+
+    def smooth(self, data):
+        """fd2d.py:349-352: Gaussian smoothing of a device field (FP64
+        [nx, pitch] tensor, or a DeviceArray); returns a float32 DeviceArray."""
+        t = data.tensor if isinstance(data, DeviceArray) else data
+        if t.dim() == 1:
+            g = self.grid
+            pad = torch.zeros((g.nx, g.pitch), dtype=torch.float64, device=self.device)
+            pad[:, : g.nz] = t.view(g.nx, g.nz).double()
+            t = pad
+        with self._ctx():
+            return DeviceArray(engine.smooth(t.double(), self.grid, int(self.config["smooth"])))

@@ -1,0 +1,113 @@
+"""Host-side logic of the b200 plugin that needs no GPU: model file
+reading and grid inference, point mapping, injection lists, shot sharding,
+and the refusal to start without CUDA."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from oracle.oracle import grid_geometry, point_ids
+from seispie_b200 import engine
+from seispie_b200.io import write_model
+from seispie_b200.solver import DeviceArray, b200
+from tests.conftest import load_golden
+
+
+def make_case_dir(tmp_path, g):
+    """Directory layout of an adjoint run for the sh_grad golden case."""
+    nx, nz = int(g["nx"]), int(g["nz"])
+    h = float(g["dx"])
+    n = nx * nz
+    true = os.path.join(str(tmp_path), "model_true")
+    init = os.path.join(str(tmp_path), "model_init")
+    write_model(true, nx, nz, h, h, dict(vp=np.full(n, 3000.0), vs=g["true_vs"], rho=np.full(n, 2600.0)))
+    write_model(init, nx, nz, h, h, dict(vp=np.full(n, 3000.0), vs=np.full(n, 1732.0), rho=np.full(n, 2600.0)))
+    out = os.path.join(str(tmp_path), "output")
+    os.makedirs(out, exist_ok=True)
+    np.savetxt(os.path.join(str(tmp_path), "src.dat"), g["src"])
+    np.savetxt(os.path.join(str(tmp_path), "rec.dat"), g["rec"])
+    return dict(model_true=true, model_init=init, sources=os.path.join(str(tmp_path), "src.dat"),
+                stations=os.path.join(str(tmp_path), "rec.dat"), output=out)
+
+
+def test_point_ids_match_reference_geometry():
+    g = load_golden("example_geometry")
+    s = b200()
+    s.nx, s.nz, s.dx, s.dz = int(g["nx"]), int(g["nz"]), g["dx"], g["dz"]
+    assert np.array_equal(s._point_ids(g["src"]), g["src_id"])
+    assert np.array_equal(s._point_ids(g["rec"]), g["rec_id"])
+    with pytest.raises(ValueError):
+        s._point_ids(np.array([[-1e9, 0.0]]))
+
+
+def test_grid_inference():
+    """Same answer as the reference's formula where that formula is
+    consistent; the right grid where it is not (1024x512, 37x5)."""
+    from seispie_b200.solver.b200 import infer_grid
+    for nx, nz in ((20, 28), (201, 201), (1024, 512), (37, 5), (512, 1024)):
+        i, j = np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij")
+        x = (i * 7.5).ravel().astype(np.float32)
+        z = (j * 7.5).ravel().astype(np.float32)
+        gx, gz, dx, dz = infer_grid(x, z, np.int32(nx * nz))
+        assert (gx, gz) == (nx, nz) and dx == np.float32(7.5) and dz == np.float32(7.5)
+        rx, rz, rdx, rdz = grid_geometry(x, z, np.int32(nx * nz))
+        if rx * rz == nx * nz:
+            assert (rx, rz, rdx, rdz) == (gx, gz, dx, dz)
+    # the reference formula itself mis-infers 1024x512
+    i, j = np.meshgrid(np.arange(1024), np.arange(512), indexing="ij")
+    assert grid_geometry((i * 10.0).ravel().astype(np.float32), (j * 10.0).ravel().astype(np.float32),
+                         np.int32(1024 * 512))[0] == 1025
+
+
+def test_injection_lists():
+    ptr, cell, row = engine.injection_lists(3, np.array([5, 9, 13]), lambda s: s)
+    assert list(ptr) == [0, 1, 2, 3] and list(cell) == [5, 9, 13] and list(row) == [0, 1, 2]
+    ptr, cell, row = engine.injection_lists(2, np.array([5, 9]), lambda s: -1)
+    assert list(ptr) == [0, 2, 4] and list(cell) == [5, 9, 5, 9] and list(row) == [0, 1, 0, 1]
+    ptr, cell, row = engine.adjoint_injection_lists(2, np.array([3, 4, 7]))
+    assert list(ptr) == [0, 3, 6] and list(cell) == [3, 4, 7, 3, 4, 7] and list(row) == list(range(6))
+
+
+def test_pitch():
+    assert [engine.pitch_for(n) for n in (1, 4, 5, 201, 512)] == [4, 4, 8, 204, 512]
+
+
+class FakeMPI:
+    def __init__(self, rank, size):
+        self._r, self._s = rank, size
+
+    def rank(self):
+        return self._r
+
+    def size(self):
+        return self._s
+
+
+def test_shot_sharding_covers_every_shot_once():
+    for nsrc in (1, 7, 12, 64):
+        for size in (1, 2, 3, 8):
+            seen = []
+            for r in range(size):
+                s = b200()
+                s.nsrc, s.mpi = nsrc, FakeMPI(r, size)
+                seen += s._shots()
+            assert sorted(seen) == list(range(nsrc))
+
+
+def test_device_array_copy_to_host():
+    t = torch.arange(12, dtype=torch.float32).view(3, 4)
+    a = DeviceArray(t, nz=3)
+    out = np.zeros(9, np.float32)
+    a.copy_to_host(out)
+    assert list(out) == [0, 1, 2, 4, 5, 6, 8, 9, 10]
+    assert a.size == 9
+
+
+@pytest.mark.skipif(torch.cuda.is_available(), reason="checks the no-GPU refusal")
+def test_setup_refuses_without_cuda():
+    s = b200()
+    s.config = dict(nt="10", dt="1e-3", sh="yes", psv="no")
+    s.path, s.mpi = {}, None
+    with pytest.raises(RuntimeError, match="CUDA"):
+        s.setup(None)
