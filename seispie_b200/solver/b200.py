@@ -38,9 +38,10 @@ class DeviceArray:
     """A device field with the numba DeviceNDArray method the upper layers
     use: ``copy_to_host(ary, stream)`` (optimize/base.py:59-61)."""
 
-    def __init__(self, tensor: torch.Tensor, nz: int | None = None):
+    def __init__(self, tensor: torch.Tensor, nz: int | None = None, stream: torch.cuda.Stream | None = None):
         self.tensor = tensor
         self.nz = nz
+        self.stream = stream  # the stream that writes the tensor; reads are ordered after it
 
     def _flat(self) -> torch.Tensor:
         t = self.tensor
@@ -53,7 +54,8 @@ class DeviceArray:
         return self._flat().numel()
 
     def copy_to_host(self, ary: np.ndarray | None = None, stream=None) -> np.ndarray:
-        with torch.cuda.stream(stream) if isinstance(stream, torch.cuda.Stream) else _nullctx():
+        s = stream if isinstance(stream, torch.cuda.Stream) else self.stream
+        with torch.cuda.stream(s) if s is not None else _nullctx():
             host = self._flat().to(torch.float32).cpu().numpy()
         if ary is None:
             return host
@@ -193,10 +195,10 @@ class b200:
                                            engine.stream_handle(self.stream)), "fwi_set_bound")
             m.prepare()
         self.model = m
-        self.rho = DeviceArray(m.rho, nz)
-        self.lam = DeviceArray(m.lam, nz)
-        self.mu = DeviceArray(m.mu, nz)
-        self.bound = DeviceArray(m.bound, nz)
+        self.rho = DeviceArray(m.rho, nz, self.stream)
+        self.lam = DeviceArray(m.lam, nz, self.stream)
+        self.mu = DeviceArray(m.mu, nz, self.stream)
+        self.bound = DeviceArray(m.bound, nz, self.stream)
         # fd2d.py:250 tests the raw string, so any non-empty value exports
         if self.config["save_coordinates"]:
             self.export_field(x, "x")
@@ -288,12 +290,12 @@ class b200:
                             self.export_field(b.field(f)[0].reshape(-1), out, last)
                 self._fwd_batches[mode] = b
                 if mode == FWI_SH:
-                    self.obs_y = DeviceArray(b.obs[1])
+                    self.obs_y = DeviceArray(b.obs[1], None, self.stream)
                 else:
-                    self.obs_x = DeviceArray(b.obs[0])
-                    self.obs_z = DeviceArray(b.obs[2])
+                    self.obs_x = DeviceArray(b.obs[0], None, self.stream)
+                    self.obs_z = DeviceArray(b.obs[2], None, self.stream)
                     if mode == FWI_SPIN:
-                        self.obs_y = DeviceArray(b.obs[1])
+                        self.obs_y = DeviceArray(b.obs[1], None, self.stream)
         if "output_traces" in self.path:
             tracedir = self.path["output_traces"]
             i = isrc if isrc >= 0 else 0
@@ -338,7 +340,8 @@ class b200:
                 for c, lst, nm in ((1, self.syn_y, "vy"), (0, self.syn_x, "vx"), (2, self.syn_z, "vz")):
                     if b.obs[c] is None or (c == 1 and mode == FWI_SPIN):
                         continue
-                    tr = b.traces(c).cpu().numpy()
+                    with self._ctx():
+                        tr = b.traces(c).cpu().numpy()
                     for q, i in enumerate(chunk):
                         out = np.ascontiguousarray(tr[q]).reshape(-1)
                         lst.append(out)
@@ -424,9 +427,9 @@ class b200:
             self._mpi_sum_kernels()
         if adj:
             with self._ctx():
-                self.k_mu = DeviceArray(engine.smooth(self.k_mu_f64, self.grid, self.sigma))
-                self.k_lam = DeviceArray(self.k_lam_f64, self.nz)
-                self.k_rho = DeviceArray(self.k_rho_f64, self.nz)
+                self.k_mu = DeviceArray(engine.smooth(self.k_mu_f64, self.grid, self.sigma), None, self.stream)
+                self.k_lam = DeviceArray(self.k_lam_f64, self.nz, self.stream)
+                self.k_rho = DeviceArray(self.k_rho_f64, self.nz, self.stream)
         if not self.mpi:
             print("  misfit = %.2f" % misfit)
         if adj:
@@ -467,10 +470,10 @@ class b200:
         """fd2d.py:349-352: Gaussian smoothing of a device field (FP64
         [nx, pitch] tensor, or a DeviceArray); returns a float32 DeviceArray."""
         t = data.tensor if isinstance(data, DeviceArray) else data
-        if t.dim() == 1:
-            g = self.grid
-            pad = torch.zeros((g.nx, g.pitch), dtype=torch.float64, device=self.device)
-            pad[:, : g.nz] = t.view(g.nx, g.nz).double()
-            t = pad
         with self._ctx():
-            return DeviceArray(engine.smooth(t.double(), self.grid, int(self.config["smooth"])))
+            if t.dim() == 1:
+                g = self.grid
+                pad = torch.zeros((g.nx, g.pitch), dtype=torch.float64, device=self.device)
+                pad[:, : g.nz] = t.view(g.nx, g.nz).double()
+                t = pad
+            return DeviceArray(engine.smooth(t.double(), self.grid, int(self.config["smooth"])), None, self.stream)
