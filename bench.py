@@ -293,22 +293,10 @@ def main():
         return mis, g
 
     def tune():
-        best = None
-        for t in _lib.tile_variants():
-            bb = ShotBatch(m_init, nshots, nt, rid, tile=t)
-            dd = bb.desc(inj=inj, stf=stf)
-            bb.clear()
-            bb.run(dd, False, 0, 20)
-            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s0.record()
-            bb.run(dd, False, 20, 100)
-            s1.record()
-            torch.cuda.synchronize()
-            ms = s0.elapsed_time(s1) / 100
-            if best is None or ms < best[1]:
-                best = (t, ms)
-            del bb
-        return best
+        from seispie_b200.autotune import autotune
+        best, times = autotune(m_init, nshots, nt, rid, inj, stf)
+        return best, times[best], {"%dx%d%s" % (*_lib.tile_shape(t), "" if t in (1, 2, 3, 4, 5) else "rw"): ms
+                                   for t, ms in times.items()}
 
     tuned = None
     if a.autotune:
@@ -378,7 +366,7 @@ def main():
     if rank == 0:
         extra = {"tile": _lib.tile_shape(b_tile(a, tuned)), "misfit": misfit_total}
         if tuned:
-            extra["autotune_ms_per_fwd_step"] = tuned[1]
+            extra["autotune_ms_per_fwd_step"] = tuned[2]
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
                 "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config_of(a, w, extra),

@@ -24,6 +24,14 @@
 // re-reads hit L2.  Velocity and stress are ping-ponged between two buffers
 // because a neighbouring tile may still be reading the old halo.
 //
+// Two compute mappings share the staging:
+//   step_kernel      any TX x TZ; each thread walks cells of the tile.
+//   step_kernel_rw   TZ = 32: lane = z, each warp owns TX/8 consecutive x
+//                    rows and keeps the x-derivative taps in a register
+//                    window sliding down x, so a row of a field is read from
+//                    shared memory once instead of four times.
+// Both do the same arithmetic per cell, so their results are bit-identical.
+//
 // Derivative masks follow solver.py:22-51 exactly: D- is zero unless
 // 2 <= i < n-2, D+ is zero unless 1 <= i < n-2 (same for j), so no value
 // outside the grid or in row padding ever reaches a result.
@@ -50,6 +58,12 @@ template <>
 struct Fields<FWI_SPIN> {
     static constexpr int NS = 6, NV = 3, NVP = 3, NIP = 4, NINJ = 2;
 };
+
+// Stress fields whose D_x^- is taken (SH: sxy; P-SV: sxx, sxz; spin also
+// syx_c, syy_c) -- these get an x register window in step_kernel_rw.
+__host__ __device__ constexpr bool takes_dxm(int mode, int f) {
+    return mode == FWI_SH ? f == 0 : (f == 0 || f == 2 || (mode == FWI_SPIN && (f == 3 || f == 4)));
+}
 
 struct StepArgs {
     int nx, nz, pitch, nt, it, nrec;
@@ -89,6 +103,25 @@ struct Tile {
     static_assert(TZ % 4 == 0, "TZ must be a multiple of 4");
 };
 
+// Shared-memory regions of one CTA.
+template <int MODE, int TX, int TZ>
+struct Smem {
+    using T = Tile<MODE, TX, TZ>;
+    float *S, *V, *P, *U, *I, *J, *val;
+    int *loc, *warp;
+    __device__ explicit Smem(float *base) {
+        S = base;
+        V = S + T::S_SZ;
+        P = V + T::V_SZ;
+        U = P + T::P_SZ;
+        I = U + T::U_SZ;
+        J = I + T::I_SZ;
+        loc = reinterpret_cast<int *>(J + T::J_SZ);
+        val = reinterpret_cast<float *>(loc + kThreads);
+        warp = reinterpret_cast<int *>(val + Fields<MODE>::NINJ * kThreads);
+    }
+};
+
 // Stage NF fields of a ROWS x COLS window starting at (gx0, gz0) into dst.
 template <int NF, int ROWS, int COLS>
 __device__ __forceinline__ void stage(float *dst, const float *const *src, long long off, int gx0, int gz0,
@@ -108,38 +141,26 @@ __device__ __forceinline__ void stage(float *dst, const float *const *src, long 
     }
 }
 
+// Staging copies plus the source scatter (stf_dsy / stf_dsxz, solver.py:78-93):
+// entries of this shot inside the computed velocity region are summed per
+// cell into sm.J, in entry order, while the copies are in flight.  Returns
+// whether the tile holds any entry (then sm.J is valid).  Ends with the
+// staged data visible to the whole CTA.
 template <int MODE, int TX, int TZ>
-__global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 2) step_kernel(const StepArgs a) {
+__device__ __forceinline__ bool prologue(const StepArgs &a, const Smem<MODE, TX, TZ> &sm, int x0, int z0, int shot) {
     using T = Tile<MODE, TX, TZ>;
     using F = Fields<MODE>;
     constexpr int SX = T::SX, SZ = T::SZ, VX = T::VX, RVZ = T::RVZ;
-    extern __shared__ __align__(16) float smem[];
-    float *sS = smem;
-    float *sV = sS + T::S_SZ;
-    float *sP = sV + T::V_SZ;
-    float *sU = sP + T::P_SZ;
-    float *sI = sU + T::U_SZ;
-    float *sJ = sI + T::I_SZ;
-    int *sLoc = reinterpret_cast<int *>(sJ + T::J_SZ);
-    float *sVal = reinterpret_cast<float *>(sLoc + kThreads);
-    int *sWarp = reinterpret_cast<int *>(sVal + F::NINJ * kThreads);
-
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int z0 = blockIdx.x * TZ, x0 = blockIdx.y * TX, shot = blockIdx.z;
     const int nx = a.nx, nz = a.nz, pitch = a.pitch;
     const long long soff = (long long)shot * nx * pitch;
-
-    // ---------------------------------------------------------------- staging
-    stage<F::NS, SX, SZ>(sS, a.sig_in, soff, x0 - 3, z0 - 4, nx, pitch, tid);
-    stage<F::NV, VX, SZ>(sV, a.vel_in, soff, x0 - 1, z0 - 4, nx, pitch, tid);
-    stage<F::NVP, VX, SZ>(sP, a.vp, 0, x0 - 1, z0 - 4, nx, pitch, tid);
-    stage<F::NV, TX, TZ>(sU, a.disp, soff, x0, z0, nx, pitch, tid);
-    stage<F::NIP, TX, TZ>(sI, a.ip, 0, x0, z0, nx, pitch, tid);
+    stage<F::NS, SX, SZ>(sm.S, a.sig_in, soff, x0 - 3, z0 - 4, nx, pitch, tid);
+    stage<F::NV, VX, SZ>(sm.V, a.vel_in, soff, x0 - 1, z0 - 4, nx, pitch, tid);
+    stage<F::NVP, VX, SZ>(sm.P, a.vp, 0, x0 - 1, z0 - 4, nx, pitch, tid);
+    stage<F::NV, TX, TZ>(sm.U, a.disp, soff, x0, z0, nx, pitch, tid);
+    stage<F::NIP, TX, TZ>(sm.I, a.ip, 0, x0, z0, nx, pitch, tid);
     cp_async_commit();
 
-    // ------------------------------------------- source scatter (stf_dsy/dsxz)
-    // Entries of this shot inside the computed velocity region are summed per
-    // cell into sJ in entry order, while the staging copies are in flight.
     bool has_inj = false;
     if (a.inj_ptr) {
         const int p0 = a.inj_ptr[shot], p1 = a.inj_ptr[shot + 1];
@@ -161,106 +182,180 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 2) step_kerne
             const int n_in = __syncthreads_count(loc >= 0);
             if (n_in == 0) continue;
             if (!has_inj) {
-                for (int q = tid; q < T::J_SZ; q += kThreads) sJ[q] = 0.f;
+                for (int q = tid; q < T::J_SZ; q += kThreads) sm.J[q] = 0.f;
                 has_inj = true;
             }
             const unsigned ball = __ballot_sync(0xffffffffu, loc >= 0);
-            if (lane == 0) sWarp[warp] = __popc(ball);
+            if (lane == 0) sm.warp[warp] = __popc(ball);
             __syncthreads();
             if (loc >= 0) {
                 int pos = __popc(ball & ((1u << lane) - 1u));
-                for (int w = 0; w < warp; w++) pos += sWarp[w];
-                sLoc[pos] = loc;
+                for (int w = 0; w < warp; w++) pos += sm.warp[w];
+                sm.loc[pos] = loc;
 #pragma unroll
-                for (int c = 0; c < F::NINJ; c++) sVal[c * kThreads + pos] = val[c];
+                for (int c = 0; c < F::NINJ; c++) sm.val[c * kThreads + pos] = val[c];
             }
             __syncthreads();
             if (tid == 0) {
                 for (int q = 0; q < n_in; q++) {
 #pragma unroll
-                    for (int c = 0; c < F::NINJ; c++) sJ[c * VX * RVZ + sLoc[q]] += sVal[c * kThreads + q];
+                    for (int c = 0; c < F::NINJ; c++) sm.J[c * VX * RVZ + sm.loc[q]] += sm.val[c * kThreads + q];
                 }
             }
             __syncthreads();
         }
     }
-
     cp_async_wait_all();
     __syncthreads();
+    return has_inj;
+}
 
-    const float cx1 = a.cx1, cx2 = a.cx2, cz1 = a.cz1, cz2 = a.cz2, dt = a.dt;
+// Velocity update of one cell from its stress divergence ds (all in shared
+// memory): v = bound * (v + ds * dt/rho)  (add_vy / add_vxz, solver.py:95-109).
+// (rx, rz): velocity-region row and computed column; writes sm.V in place.
+template <int MODE, int TX, int TZ>
+__device__ __forceinline__ void velocity_update(const Smem<MODE, TX, TZ> &sm, int rx, int rz, float (&ds)[3],
+                                                bool has_inj, float (&vnew)[3]) {
+    using T = Tile<MODE, TX, TZ>;
+    using F = Fields<MODE>;
+    constexpr int SZ = T::SZ, VX = T::VX, RVZ = T::RVZ;
+    if (has_inj) {
+#pragma unroll
+        for (int c = 0; c < F::NINJ; c++) ds[c] += sm.J[c * VX * RVZ + rx * RVZ + rz];
+    }
+    const int vi = rx * SZ + rz + 3;
+    const float buo = sm.P[vi], bnd = sm.P[VX * SZ + vi];
+#pragma unroll
+    for (int c = 0; c < F::NV; c++) {
+        const float b = (MODE == FWI_SPIN && c == 2) ? sm.P[2 * VX * SZ + vi] : buo;
+        const float v = bnd * (sm.V[c * VX * SZ + vi] + ds[c] * b);
+        sm.V[c * VX * SZ + vi] = v;
+        vnew[c] = v;
+    }
+}
 
-    // ------------------------------------------------------- velocity half
-    // (rx, rz): velocity row / computed column; returns true if inside grid.
-    auto velocity = [&](int rx, int rz, float *vnew) -> bool {
-        const int gx = x0 - 1 + rx, gz = z0 - 1 + rz;
-        const int cz = rz + 3, vi = rx * SZ + cz;
-        if (gx < 0 || gx >= nx || gz < 0 || gz >= nz) {
-#pragma unroll
-            for (int c = 0; c < F::NV; c++) sV[c * VX * SZ + vi] = 0.f;
-            return false;
-        }
-        const bool okx = gx >= 2 && gx < nx - 2, okz = gz >= 2 && gz < nz - 2;
-        const float *s0 = sS + (rx + 2) * SZ + cz;
-        auto dxm = [&](int f) -> float {
-            if (!okx) return 0.f;
-            const float *s = s0 + f * SX * SZ;
-            return cx1 * (s[0] - s[-SZ]) - cx2 * (s[SZ] - s[-2 * SZ]);
-        };
-        auto dzm = [&](int f) -> float {
-            if (!okz) return 0.f;
-            const float *s = s0 + f * SX * SZ;
-            return cz1 * (s[0] - s[-1]) - cz2 * (s[1] - s[-2]);
-        };
-        float ds[F::NV];
-        if (MODE == FWI_SH) {
-            ds[0] = dxm(0) + dzm(1);
-        } else {
-            ds[0] = dxm(0) + dzm(2);
-            ds[1] = dxm(2) + dzm(1);
-            if (MODE == FWI_SPIN) {
-                ds[0] += dzm(4);
-                ds[1] -= dxm(4);
-                ds[2] = (dxm(3) + dzm(5)) + 2.f * s0[4 * SX * SZ];
-            }
-        }
-        if (has_inj) {
-#pragma unroll
-            for (int c = 0; c < F::NINJ; c++) ds[c] += sJ[c * VX * RVZ + rx * RVZ + rz];
-        }
-        const float buo = sP[vi], bnd = sP[VX * SZ + vi];
-#pragma unroll
-        for (int c = 0; c < F::NV; c++) {
-            const float b = (MODE == FWI_SPIN && c == 2) ? sP[2 * VX * SZ + vi] : buo;
-            const float v = bnd * (sV[c * VX * SZ + vi] + ds[c] * b);
-            sV[c * VX * SZ + vi] = v;
-            vnew[c] = v;
-        }
-        return true;
-    };
-
-    const long long tile_off = soff;
-    // interior cells: also write v, u, snapshots
-    for (int c = tid; c < TX * TZ; c += kThreads) {
-        const int ix = c / TZ, iz = c - ix * TZ;
-        float v[F::NV];
-        if (velocity(ix + 1, iz + 1, v)) {
-            const long long g = tile_off + (long long)(x0 + ix) * pitch + (z0 + iz);
-#pragma unroll
-            for (int q = 0; q < F::NV; q++) {
-                const float u = sU[q * TX * TZ + c] + v[q] * dt;
-                sU[q * TX * TZ + c] = u;
-                a.vel_out[q][g] = v[q];
-                a.disp[q][g] = u;
-                if (a.snap_u[q]) a.snap_u[q][g] = u;
-                if (a.snap_v[q]) a.snap_v[q][g] = v[q];
-            }
+// Stress divergence of one cell (div_sy / div_sxz / div_sxyz_c,
+// solver.py:54-75) from D_x^- and D_z^- values supplied by the caller.
+template <int MODE, class DXM, class DZM, class CEN>
+__device__ __forceinline__ void divergence(DXM dxm, DZM dzm, CEN center, float (&ds)[3]) {
+    if (MODE == FWI_SH) {
+        ds[0] = dxm(0) + dzm(1);
+    } else {
+        ds[0] = dxm(0) + dzm(2);
+        ds[1] = dxm(2) + dzm(1);
+        if (MODE == FWI_SPIN) {
+            ds[0] += dzm(4);
+            ds[1] -= dxm(4);
+            ds[2] = (dxm(3) + dzm(5)) + 2.f * center(4);
         }
     }
-    // halo cells of the velocity region: rows x0-1, x0+TX, x0+TX+1 (all
-    // columns) and columns z0-1, z0+TZ, z0+TZ+1 of the interior rows
+}
+
+// Stress update of one interior cell (add_sy / add_sxz / add_sy_c,
+// solver.py:128-149) from D+ of the new velocity; s0 points at the cell's
+// old stress in shared memory, ip at its stiffness, g is its HBM offset.
+template <int MODE, int TX, int TZ, class DXP, class DZP>
+__device__ __forceinline__ void stress_update(const StepArgs &a, const float *s0, const float *ip, float vyc, long long g,
+                                              DXP dxp, DZP dzp) {
+    using T = Tile<MODE, TX, TZ>;
+    constexpr int FS = T::SX * T::SZ, FI = TX * TZ;
+    const float dt = a.dt;
+    if (MODE == FWI_SH) {
+        const float dm = dt * ip[0];
+        a.sig_out[0][g] = s0[0] + dm * dxp(0);
+        a.sig_out[1][g] = s0[FS] + dm * dzp(0);
+    } else {
+        const float lam = ip[0], mu = ip[FI];
+        const float vxx = dxp(0), vxz = dzp(0), vzx = dxp(1), vzz = dzp(1);
+        const float l2m = lam + 2.f * mu;
+        a.sig_out[0][g] = s0[0] + dt * (l2m * vxx + lam * vzz);
+        a.sig_out[1][g] = s0[FS] + dt * (l2m * vzz + lam * vxx);
+        a.sig_out[2][g] = s0[2 * FS] + dt * (mu * (vxz + vzx));
+        if (MODE == FWI_SPIN) {
+            const float nu = ip[2 * FI], mnc = ip[3 * FI];
+            a.sig_out[4][g] = s0[4 * FS] + a.dt2 * nu * (-vyc - 0.5f * (vzx - vxz));
+            a.sig_out[3][g] = s0[3 * FS] + dt * mnc * dxp(2);
+            a.sig_out[5][g] = s0[5 * FS] + dt * mnc * dzp(2);
+        }
+    }
+}
+
+// Interior bookkeeping after a velocity update: HBM writes of v and u,
+// snapshots, u into shared memory for the receivers.
+template <int MODE, int TX, int TZ>
+__device__ __forceinline__ void store_interior(const StepArgs &a, const Smem<MODE, TX, TZ> &sm, int ci, long long g,
+                                               const float (&v)[3]) {
+#pragma unroll
+    for (int q = 0; q < Fields<MODE>::NV; q++) {
+        const float u = sm.U[q * TX * TZ + ci] + v[q] * a.dt;
+        sm.U[q * TX * TZ + ci] = u;
+        a.vel_out[q][g] = v[q];
+        a.disp[q][g] = u;
+        if (a.snap_u[q]) a.snap_u[q][g] = u;
+        if (a.snap_v[q]) a.snap_v[q][g] = v[q];
+    }
+}
+
+// Receivers of this tile record the new displacement (save_obs).
+template <int MODE, int TX, int TZ>
+__device__ __forceinline__ void gather_receivers(const StepArgs &a, const Smem<MODE, TX, TZ> &sm, int x0, int z0,
+                                                 int shot) {
+    if (!a.rec_cell) return;
+    for (int r = threadIdx.x; r < a.nrec; r += kThreads) {
+        const int k = a.rec_cell[r];
+        const int gx = fdiv(k, a.divnz), gz = k - gx * a.nz;
+        const int ix = gx - x0, iz = gz - z0;
+        if (ix >= 0 && ix < TX && iz >= 0 && iz < TZ) {
+            const long long o = ((long long)shot * a.nrec + r) * a.nt + a.it;
+#pragma unroll
+            for (int q = 0; q < Fields<MODE>::NV; q++)
+                if (a.obs[q]) a.obs[q][o] = sm.U[q * TX * TZ + ix * TZ + iz];
+        }
+    }
+}
+
+// Velocity of one cell of the computed region, generic path (all loads from
+// shared memory).  Returns false for a cell outside the grid (v set to 0).
+template <int MODE, int TX, int TZ>
+__device__ __forceinline__ bool velocity_cell(const StepArgs &a, const Smem<MODE, TX, TZ> &sm, int x0, int z0, int rx,
+                                              int rz, bool has_inj, float (&v)[3]) {
+    using T = Tile<MODE, TX, TZ>;
+    constexpr int SX = T::SX, SZ = T::SZ, VX = T::VX;
+    const int gx = x0 - 1 + rx, gz = z0 - 1 + rz;
+    const int cz = rz + 3;
+    if (gx < 0 || gx >= a.nx || gz < 0 || gz >= a.nz) {
+#pragma unroll
+        for (int c = 0; c < Fields<MODE>::NV; c++) sm.V[c * VX * SZ + rx * SZ + cz] = 0.f;
+        return false;
+    }
+    const bool okx = gx >= 2 && gx < a.nx - 2, okz = gz >= 2 && gz < a.nz - 2;
+    const float *s0 = sm.S + (rx + 2) * SZ + cz;
+    const float cx1 = a.cx1, cx2 = a.cx2, cz1 = a.cz1, cz2 = a.cz2;
+    auto dxm = [&](int f) -> float {
+        if (!okx) return 0.f;
+        const float *s = s0 + f * SX * SZ;
+        return cx1 * (s[0] - s[-SZ]) - cx2 * (s[SZ] - s[-2 * SZ]);
+    };
+    auto dzm = [&](int f) -> float {
+        if (!okz) return 0.f;
+        const float *s = s0 + f * SX * SZ;
+        return cz1 * (s[0] - s[-1]) - cz2 * (s[1] - s[-2]);
+    };
+    auto center = [&](int f) -> float { return s0[f * SX * SZ]; };
+    float ds[3];
+    divergence<MODE>(dxm, dzm, center, ds);
+    velocity_update<MODE, TX, TZ>(sm, rx, rz, ds, has_inj, v);
+    return true;
+}
+
+// Halo cells of the velocity region: rows x0-1, x0+TX, x0+TX+1 (all columns)
+// and columns z0-1, z0+TZ, z0+TZ+1 of the interior rows.
+template <int MODE, int TX, int TZ>
+__device__ __forceinline__ void velocity_halo(const StepArgs &a, const Smem<MODE, TX, TZ> &sm, int x0, int z0,
+                                              bool has_inj) {
+    constexpr int RVZ = Tile<MODE, TX, TZ>::RVZ;
     constexpr int HROW = 3 * RVZ, HC = HROW + 3 * TX;
-    for (int c = tid; c < HC; c += kThreads) {
+    for (int c = threadIdx.x; c < HC; c += kThreads) {
         int rx, rz;
         if (c < HROW) {
             const int r3 = c / RVZ;
@@ -271,33 +366,41 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 2) step_kerne
             rx = 1 + c2 / 3;
             rz = k3 == 0 ? 0 : TZ + k3;
         }
-        float v[F::NV];
-        velocity(rx, rz, v);
+        float v[3];
+        velocity_cell<MODE, TX, TZ>(a, sm, x0, z0, rx, rz, has_inj, v);
     }
+}
+
+// ------------------------------------------------------- generic mapping
+
+template <int MODE, int TX, int TZ>
+__global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 2) step_kernel(const StepArgs a) {
+    using T = Tile<MODE, TX, TZ>;
+    constexpr int SX = T::SX, SZ = T::SZ, VX = T::VX;
+    extern __shared__ __align__(16) float smem[];
+    const Smem<MODE, TX, TZ> sm(smem);
+    const int z0 = blockIdx.x * TZ, x0 = blockIdx.y * TX, shot = blockIdx.z;
+    const int nx = a.nx, nz = a.nz, pitch = a.pitch;
+    const long long soff = (long long)shot * nx * pitch;
+    const bool has_inj = prologue<MODE, TX, TZ>(a, sm, x0, z0, shot);
+
+    for (int c = threadIdx.x; c < TX * TZ; c += kThreads) {
+        const int ix = c / TZ, iz = c - ix * TZ;
+        float v[3];
+        if (velocity_cell<MODE, TX, TZ>(a, sm, x0, z0, ix + 1, iz + 1, has_inj, v))
+            store_interior<MODE, TX, TZ>(a, sm, c, soff + (long long)(x0 + ix) * pitch + (z0 + iz), v);
+    }
+    velocity_halo<MODE, TX, TZ>(a, sm, x0, z0, has_inj);
     __syncthreads();
+    gather_receivers<MODE, TX, TZ>(a, sm, x0, z0, shot);
 
-    // ------------------------------------------------ receivers (save_obs)
-    if (a.rec_cell) {
-        for (int r = tid; r < a.nrec; r += kThreads) {
-            const int k = a.rec_cell[r];
-            const int gx = fdiv(k, a.divnz), gz = k - gx * nz;
-            const int ix = gx - x0, iz = gz - z0;
-            if (ix >= 0 && ix < TX && iz >= 0 && iz < TZ) {
-                const long long o = ((long long)shot * a.nrec + r) * a.nt + a.it;
-#pragma unroll
-                for (int q = 0; q < F::NV; q++)
-                    if (a.obs[q]) a.obs[q][o] = sU[q * TX * TZ + ix * TZ + iz];
-            }
-        }
-    }
-
-    // --------------------------------------------------------- stress half
-    for (int c = tid; c < TX * TZ; c += kThreads) {
+    const float cx1 = a.cx1, cx2 = a.cx2, cz1 = a.cz1, cz2 = a.cz2;
+    for (int c = threadIdx.x; c < TX * TZ; c += kThreads) {
         const int ix = c / TZ, iz = c - ix * TZ;
         const int gx = x0 + ix, gz = z0 + iz;
         if (gx >= nx || gz >= nz) continue;
         const bool okx = gx >= 1 && gx < nx - 2, okz = gz >= 1 && gz < nz - 2;
-        const float *v0 = sV + (ix + 1) * SZ + (iz + 4);
+        const float *v0 = sm.V + (ix + 1) * SZ + (iz + 4);
         auto dxp = [&](int f) -> float {
             if (!okx) return 0.f;
             const float *v = v0 + f * VX * SZ;
@@ -308,26 +411,102 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 2) step_kerne
             const float *v = v0 + f * VX * SZ;
             return cz1 * (v[1] - v[0]) - cz2 * (v[2] - v[-1]);
         };
-        const float *s0 = sS + (ix + 3) * SZ + (iz + 4);
-        const long long g = tile_off + (long long)gx * pitch + gz;
-        if (MODE == FWI_SH) {
-            const float dm = dt * sI[c];
-            a.sig_out[0][g] = s0[0] + dm * dxp(0);
-            a.sig_out[1][g] = s0[SX * SZ] + dm * dzp(0);
-        } else {
-            const float lam = sI[c], mu = sI[TX * TZ + c];
-            const float vxx = dxp(0), vxz = dzp(0), vzx = dxp(1), vzz = dzp(1);
-            const float l2m = lam + 2.f * mu;
-            a.sig_out[0][g] = s0[0] + dt * (l2m * vxx + lam * vzz);
-            a.sig_out[1][g] = s0[SX * SZ] + dt * (l2m * vzz + lam * vxx);
-            a.sig_out[2][g] = s0[2 * SX * SZ] + dt * (mu * (vxz + vzx));
-            if (MODE == FWI_SPIN) {
-                const float nu = sI[2 * TX * TZ + c], mnc = sI[3 * TX * TZ + c];
-                const float vyc = v0[2 * VX * SZ];
-                a.sig_out[4][g] = s0[4 * SX * SZ] + a.dt2 * nu * (-vyc - 0.5f * (vzx - vxz));
-                a.sig_out[3][g] = s0[3 * SX * SZ] + dt * mnc * dxp(2);
-                a.sig_out[5][g] = s0[5 * SX * SZ] + dt * mnc * dzp(2);
+        const float vyc = MODE == FWI_SPIN ? v0[2 * VX * SZ] : 0.f;
+        stress_update<MODE, TX, TZ>(a, sm.S + (ix + 3) * SZ + (iz + 4), sm.I + c, vyc,
+                                    soff + (long long)gx * pitch + gz, dxp, dzp);
+    }
+    (void)SX;
+}
+
+// -------------------------------------------------- register-window mapping
+
+template <int MODE, int TX>
+__global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 3) step_kernel_rw(const StepArgs a) {
+    constexpr int TZ = 32, RPW = TX / (kThreads / 32);
+    static_assert(RPW >= 1 && RPW * (kThreads / 32) == TX, "TX must be a multiple of the warp count");
+    using T = Tile<MODE, TX, TZ>;
+    using F = Fields<MODE>;
+    constexpr int SX = T::SX, SZ = T::SZ, VX = T::VX;
+    extern __shared__ __align__(16) float smem[];
+    const Smem<MODE, TX, TZ> sm(smem);
+    const int z0 = blockIdx.x * TZ, x0 = blockIdx.y * TX, shot = blockIdx.z;
+    const int nx = a.nx, nz = a.nz, pitch = a.pitch;
+    const long long soff = (long long)shot * nx * pitch;
+    const bool has_inj = prologue<MODE, TX, TZ>(a, sm, x0, z0, shot);
+
+    const int lane = threadIdx.x & 31, ix0 = (threadIdx.x >> 5) * RPW;
+    const int gz = z0 + lane, col = lane + 4;
+    const bool zin = gz < nz;
+    const float cx1 = a.cx1, cx2 = a.cx2, cz1 = a.cz1, cz2 = a.cz2;
+
+    // ---- velocity on the warp's interior rows: S rows ix0+1 .. ix0+RPW+3 of
+    // the D_x^- fields sit in registers (window index q <-> S row ix0+1+q)
+    {
+        const bool okz = gz >= 2 && gz < nz - 2;
+        float w[F::NS][RPW + 3];
+#pragma unroll
+        for (int f = 0; f < F::NS; f++)
+            if (takes_dxm(MODE, f)) {
+#pragma unroll
+                for (int r = 0; r < RPW + 3; r++) w[f][r] = sm.S[f * SX * SZ + (ix0 + 1 + r) * SZ + col];
             }
+#pragma unroll
+        for (int q = 0; q < RPW; q++) {
+            const int ix = ix0 + q, gx = x0 + ix;
+            const int vi = (ix + 1) * SZ + col;
+            if (!(zin && gx < nx)) {
+#pragma unroll
+                for (int c = 0; c < F::NV; c++) sm.V[c * VX * SZ + vi] = 0.f;
+                continue;
+            }
+            const bool okx = gx >= 2 && gx < nx - 2;
+            const float *srow = sm.S + (ix + 3) * SZ + col;
+            auto dxm = [&](int f) -> float {
+                return okx ? cx1 * (w[f][q + 2] - w[f][q + 1]) - cx2 * (w[f][q + 3] - w[f][q]) : 0.f;
+            };
+            auto center = [&](int f) -> float { return takes_dxm(MODE, f) ? w[f][q + 2] : srow[f * SX * SZ]; };
+            auto dzm = [&](int f) -> float {
+                if (!okz) return 0.f;
+                const float *s = srow + f * SX * SZ;
+                return cz1 * (center(f) - s[-1]) - cz2 * (s[1] - s[-2]);
+            };
+            float ds[3], v[3];
+            divergence<MODE>(dxm, dzm, center, ds);
+            velocity_update<MODE, TX, TZ>(sm, ix + 1, lane + 1, ds, has_inj, v);
+            store_interior<MODE, TX, TZ>(a, sm, ix * TZ + lane, soff + (long long)gx * pitch + gz, v);
+        }
+    }
+    velocity_halo<MODE, TX, TZ>(a, sm, x0, z0, has_inj);
+    __syncthreads();
+    gather_receivers<MODE, TX, TZ>(a, sm, x0, z0, shot);
+
+    // ---- stress on the same rows: V rows ix0 .. ix0+RPW+2 in registers
+    // (window index q <-> V row ix0+q; the cell of row ix is V row ix+1)
+    {
+        const bool okz = gz >= 1 && gz < nz - 2;
+        float w[F::NV][RPW + 3];
+#pragma unroll
+        for (int f = 0; f < F::NV; f++) {
+#pragma unroll
+            for (int r = 0; r < RPW + 3; r++) w[f][r] = sm.V[f * VX * SZ + (ix0 + r) * SZ + col];
+        }
+#pragma unroll
+        for (int q = 0; q < RPW; q++) {
+            const int ix = ix0 + q, gx = x0 + ix;
+            if (!(zin && gx < nx)) continue;
+            const bool okx = gx >= 1 && gx < nx - 2;
+            const float *vrow = sm.V + (ix + 1) * SZ + col;
+            auto dxp = [&](int f) -> float {
+                return okx ? cx1 * (w[f][q + 2] - w[f][q + 1]) - cx2 * (w[f][q + 3] - w[f][q]) : 0.f;
+            };
+            auto dzp = [&](int f) -> float {
+                if (!okz) return 0.f;
+                const float *v = vrow + f * VX * SZ;
+                return cz1 * (v[1] - w[f][q + 1]) - cz2 * (v[2] - v[-1]);
+            };
+            const float vyc = MODE == FWI_SPIN ? w[F::NV - 1][q + 1] : 0.f;
+            stress_update<MODE, TX, TZ>(a, sm.S + (ix + 3) * SZ + col, sm.I + ix * TZ + lane, vyc,
+                                        soff + (long long)gx * pitch + gz, dxp, dzp);
         }
     }
 }
@@ -335,36 +514,46 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 2) step_kerne
 // ------------------------------------------------------------- launching
 
 struct TileShape {
-    int tx, tz;
+    int tx, tz, rw;
 };
-// tile variants selectable through fwi_batch.tile (0 = default)
-static const TileShape kTiles[] = {{32, 32}, {32, 32}, {16, 64}, {16, 32}, {64, 32}, {8, 64}};
+// Variants selectable through fwi_batch.tile; 0 is the default.
+static const TileShape kTiles[] = {{32, 32, 1}, {32, 32, 0}, {16, 64, 0}, {16, 32, 0}, {64, 32, 0},
+                                   {8, 64, 0},  {32, 32, 1}, {16, 32, 1}, {64, 32, 1}};
 constexpr int kNumTiles = sizeof(kTiles) / sizeof(kTiles[0]);
 
-template <int MODE, int TX, int TZ>
+template <int MODE, int TX, int TZ, bool RW>
 static int launch_tile(const StepArgs &a, int nshots, cudaStream_t st) {
     using T = Tile<MODE, TX, TZ>;
+    void (*kern)(const StepArgs);
+    if constexpr (RW) {
+        static_assert(TZ == 32, "the register-window mapping has one lane per z column");
+        kern = step_kernel_rw<MODE, TX>;
+    } else {
+        kern = step_kernel<MODE, TX, TZ>;
+    }
     static bool attr_set = false;
     if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(step_kernel<MODE, TX, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)T::bytes);
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::bytes);
         if (e != cudaSuccess) return set_error(FWI_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
         attr_set = true;
     }
     dim3 grid((a.nz + TZ - 1) / TZ, (a.nx + TX - 1) / TX, nshots);
-    step_kernel<MODE, TX, TZ><<<grid, kThreads, T::bytes, st>>>(a);
+    kern<<<grid, kThreads, T::bytes, st>>>(a);
     return check_launch("step_kernel");
 }
 
 template <int MODE>
 static int launch_mode(const StepArgs &a, int nshots, int tile, cudaStream_t st) {
     switch (tile) {
-        case 0:
-        case 1: return launch_tile<MODE, 32, 32>(a, nshots, st);
-        case 2: return launch_tile<MODE, 16, 64>(a, nshots, st);
-        case 3: return launch_tile<MODE, 16, 32>(a, nshots, st);
-        case 4: return launch_tile<MODE, 64, 32>(a, nshots, st);
-        case 5: return launch_tile<MODE, 8, 64>(a, nshots, st);
+        case 0: return launch_tile<MODE, 32, 32, true>(a, nshots, st);
+        case 1: return launch_tile<MODE, 32, 32, false>(a, nshots, st);
+        case 2: return launch_tile<MODE, 16, 64, false>(a, nshots, st);
+        case 3: return launch_tile<MODE, 16, 32, false>(a, nshots, st);
+        case 4: return launch_tile<MODE, 64, 32, false>(a, nshots, st);
+        case 5: return launch_tile<MODE, 8, 64, false>(a, nshots, st);
+        case 6: return launch_tile<MODE, 32, 32, true>(a, nshots, st);
+        case 7: return launch_tile<MODE, 16, 32, true>(a, nshots, st);
+        case 8: return launch_tile<MODE, 64, 32, true>(a, nshots, st);
     }
     return set_error(FWI_EINVAL, "unknown tile variant %d", tile);
 }
@@ -376,22 +565,6 @@ bool tile_shape(int tile, int *tx, int *tz) {
     *tx = kTiles[tile].tx;
     *tz = kTiles[tile].tz;
     return true;
-}
-
-size_t step_smem_bytes(int mode, int tile) {
-    if (tile < 0 || tile >= kNumTiles) return 0;
-    const TileShape t = kTiles[tile];
-#define SMEM_CASE(M)                                                       \
-    if (t.tx == 32 && t.tz == 32) return Tile<M, 32, 32>::bytes;           \
-    if (t.tx == 16 && t.tz == 64) return Tile<M, 16, 64>::bytes;           \
-    if (t.tx == 16 && t.tz == 32) return Tile<M, 16, 32>::bytes;           \
-    if (t.tx == 64 && t.tz == 32) return Tile<M, 64, 32>::bytes;           \
-    if (t.tx == 8 && t.tz == 64) return Tile<M, 8, 64>::bytes;
-    if (mode == FWI_SH) { SMEM_CASE(FWI_SH) }
-    if (mode == FWI_PSV) { SMEM_CASE(FWI_PSV) }
-    if (mode == FWI_SPIN) { SMEM_CASE(FWI_SPIN) }
-#undef SMEM_CASE
-    return 0;
 }
 
 // Fill the per-step arguments shared by every step of a run.
