@@ -169,6 +169,24 @@ int fwi_misfit(const float *data, const float *syn, float *adstf, double *misfit
                double *partial, int nshots, int nrec, int nt, double dt, void *stream);
 long long fwi_misfit_partials(int nrec, int nt);
 
+/* Capacity, in FP64 partial sums, of the fixed scratch of fwi_misfit_noalloc
+ * (1 MiB): nshots * fwi_misfit_partials(nrec, nt) must not exceed it. */
+#define FWI_MISFIT_NOALLOC_MAX_PARTIALS (1 << 17)
+
+/* fwi_misfit for callers that cannot allocate device memory while they run
+ * (an application whose pool owns all device memory after start-up, or a
+ * time-critical loop where cudaMalloc/cudaFree would synchronise the device):
+ * same arguments and results as fwi_misfit minus `partial`, whose role is
+ * taken by a fixed array inside the library (FWI_MISFIT_NOALLOC_MAX_PARTIALS
+ * doubles on every device that loads the library, until exit).  Larger
+ * batches are rejected with FWI_ERANGE.  The first call on a device looks up
+ * the array's address (that device current); make it outside stream capture.
+ * All calls share the array: calls that overlap on the GPU race, so keep them
+ * in order on one stream.  It allocates nothing.  No counterpart in the
+ * reference. */
+int fwi_misfit_noalloc(const float *data, const float *syn, float *adstf, double *misfit, int nshots, int nrec,
+                       int nt, double dt, void *stream);
+
 /* Separable Gaussian smoothing of an FP64 kernel ([nx][in_pitch]) into a
  * float32 field ([nx][out_pitch]), normalised by the Gaussian mass inside
  * the grid as init_gausian does; taps beyond 6 sigma (relative weight

@@ -74,6 +74,8 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
         "fwi_misfit": ([_vp, _vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _vp],
                        ctypes.c_int),
         "fwi_misfit_partials": ([ctypes.c_int, ctypes.c_int], ctypes.c_longlong),
+        "fwi_misfit_noalloc": ([_vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _vp],
+                               ctypes.c_int),
         "fwi_smooth": ([_vp, ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp],
                        ctypes.c_int),
     }

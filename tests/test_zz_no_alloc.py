@@ -1,0 +1,59 @@
+"""fwi_misfit_noalloc: the misfit entry point for callers that cannot
+allocate device memory while they run (an application whose own pool owns the
+device memory after start-up, or a time-critical loop where cudaMalloc /
+cudaFree would synchronise the device).  It keeps its reduction scratch in a
+fixed array inside the library instead of a caller buffer.
+
+Checked through the C-ABI against fwi_misfit (which takes caller scratch) on
+two calls in a row with different data and sizes, so the second call runs on
+the scratch the first one left behind.  This file is collected last.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from seispie_b200 import _lib
+
+
+def _call_pair(torch, lib, rng, nshots, nrec, nt, dt):
+    data = torch.as_tensor(rng.standard_normal(nshots * nrec * nt).astype(np.float32)).cuda()
+    syn = torch.as_tensor(rng.standard_normal(nshots * nrec * nt).astype(np.float32)).cuda()
+    ad_ref = torch.empty_like(data)
+    ad_new = torch.full_like(data, float("nan"))
+    m_ref = torch.zeros(nshots, dtype=torch.float64, device="cuda")
+    m_new = torch.full((nshots,), float("nan"), dtype=torch.float64, device="cuda")
+    part = torch.empty(nshots * lib.fwi_misfit_partials(nrec, nt), dtype=torch.float64, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream or None
+    _lib.check(lib.fwi_misfit(data.data_ptr(), syn.data_ptr(), ad_ref.data_ptr(), m_ref.data_ptr(), part.data_ptr(),
+                              nshots, nrec, nt, dt, s), "fwi_misfit")
+    _lib.check(lib.fwi_misfit_noalloc(data.data_ptr(), syn.data_ptr(), ad_new.data_ptr(), m_new.data_ptr(), nshots,
+                                      nrec, nt, dt, s), "fwi_misfit_noalloc")
+    torch.cuda.synchronize()
+    return ad_ref.cpu().numpy(), ad_new.cpu().numpy(), m_ref.cpu().numpy(), m_new.cpu().numpy()
+
+
+@pytest.mark.gpu
+def test_misfit_noalloc_matches_fwi_misfit_twice():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    lib = _lib.load()
+    rng = np.random.default_rng(42)
+    for nshots, nrec, nt, dt in ((3, 7, 700, 2e-3), (2, 11, 1300, 1e-3)):
+        ad_ref, ad_new, m_ref, m_new = _call_pair(torch, lib, rng, nshots, nrec, nt, dt)
+        assert np.array_equal(ad_new, ad_ref)  # the adjoint source is bit-exact in every test of this library
+        assert np.all(np.abs(m_new / m_ref - 1) < 1e-6)
+
+
+def test_misfit_noalloc_rejects_batches_beyond_its_scratch():
+    """Rejected on the host before any CUDA call (runs without a GPU)."""
+    lib = _lib.load()
+    cap = 1 << 17
+    nt = 256 * 64
+    nrec = cap // 64 + 1  # one shot: nrec * 64 partial sums > cap
+    rc = lib.fwi_misfit_noalloc(8, 8, 8, 8, 1, nrec, nt, 1e-3, None)
+    assert rc == -3
+    buf = ctypes.create_string_buffer(512)
+    lib.fwi_last_error(buf, 512)
+    assert b"partial sums" in buf.value and b"fwi_misfit" in buf.value
