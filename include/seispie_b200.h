@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define FWI_ABI_VERSION 1
+#define FWI_ABI_VERSION 2
 
 /* status codes */
 #define FWI_OK 0
@@ -99,6 +99,14 @@ typedef struct fwi_batch {
     float *snap_u[3];
     float *snap_v[3];
     double *k_lam, *k_mu, *k_rho;
+    /* Exact discrete adjoint (fwi_run_transposed).  Forward runs with these
+     * set also store, for every step it with 0 <= it-seg0 < nseg, the new
+     * velocity v(it+1) into seg_v[c] and the stress divergence including the
+     * sources of step it into seg_ds[c], at slot it-seg0 of
+     * [nseg][nshots][nx][pitch] buffers (component slots as obs).  NULL skips. */
+    float *seg_v[3];
+    float *seg_ds[3];
+    int seg0, nseg;
 } fwi_batch;
 
 /* ABI version of the loaded library (FWI_ABI_VERSION). */
@@ -157,6 +165,21 @@ int fwi_prepare_model(const float *rho, const float *j, const float *mu_c, const
  * The caller clears the wavefields first (fwi_clear or cudaMemsetAsync),
  * as clear_wavefields does (fd2d.py:318-341).  b->cur is updated. */
 int fwi_run(fwi_batch *b, int adjoint, int it0, int nsteps, void *stream);
+
+/* Exact discrete adjoint of fwi_run's SH / P-SV forward step, run backwards
+ * over forward steps it = it_hi-1 down to it_hi-nsteps on the adjoint state
+ * held in the batch's wavefield buffers (sig~, v~, u~; cleared by the caller
+ * before the last step).  Before transposing step it, the trace gradients
+ * stf_c[inj_row[e]*nt + it] (dL/d trace in forward time order; rows as for
+ * fwi_run's injection, typically one per receiver and shot) are added to u~
+ * at inj_cell[e].  Each step also accumulates, over every shot, into the FP64
+ * arrays: dL/dlam (k_lam, P-SV), dL/dmu (k_mu), dL/dbuo with buo = dt/rho
+ * (k_rho).  Needs the forward v(it+1) and divergence of step it in seg_v /
+ * seg_ds for every step of the range (written by a forward fwi_run over the
+ * same segment).  No counterpart in the reference, whose adjoint
+ * (solver.py:290-329) is the continuous-adjoint approximation fwi_run's
+ * adjoint = 1 reproduces. */
+int fwi_run_transposed(fwi_batch *b, int it_hi, int nsteps, void *stream);
 
 /* L2 waveform misfit and adjoint source for nshots x nrec traces of nt
  * samples (receiver-major, [shot][rec][t]).  data = observed traces (the

@@ -13,7 +13,7 @@ from . import build as _build
 
 FWI_SH, FWI_PSV, FWI_SPIN = 0, 1, 2
 MODES = {"sh": FWI_SH, "psv": FWI_PSV, "spin": FWI_SPIN}
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 _fp = ctypes.POINTER(ctypes.c_float)
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -33,6 +33,7 @@ class FwiBatch(ctypes.Structure):
         ("nrec", ctypes.c_int), ("rec_cell", _vp), ("obs", _vp * 3),
         ("sae", ctypes.c_int), ("nsa", ctypes.c_int), ("snap_u", _vp * 3), ("snap_v", _vp * 3),
         ("k_lam", _vp), ("k_mu", _vp), ("k_rho", _vp),
+        ("seg_v", _vp * 3), ("seg_ds", _vp * 3), ("seg0", ctypes.c_int), ("nseg", ctypes.c_int),
     ]
 
 
@@ -71,6 +72,7 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
         "fwi_prepare_model": ([_vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_longlong, _vp, _vp, _vp, _vp],
                               ctypes.c_int),
         "fwi_run": ([ctypes.POINTER(FwiBatch), ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp], ctypes.c_int),
+        "fwi_run_transposed": ([ctypes.POINTER(FwiBatch), ctypes.c_int, ctypes.c_int, _vp], ctypes.c_int),
         "fwi_misfit": ([_vp, _vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _vp],
                        ctypes.c_int),
         "fwi_misfit_partials": ([ctypes.c_int, ctypes.c_int], ctypes.c_longlong),

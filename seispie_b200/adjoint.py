@@ -1,0 +1,203 @@
+"""Exact gradients of seismograms with respect to the model, and the
+``torch.autograd.Function`` around them.
+
+The forward is the fused step (``fwi_run``); the backward is its exact
+discrete transpose (``fwi_run_transposed``), which needs, for every step, the
+forward velocity after the step and the stress divergence of the step.  Those
+are recomputed segment by segment from checkpoints of the full wavefield
+taken every ``K`` steps during the forward pass (uniform checkpointing): the
+memory is ``nt/K`` wavefield copies plus ``K`` steps of velocity and
+divergence, the cost one extra forward sweep.  ``K`` defaults to the value
+that balances the two, shrunk further to fit the memory budget.
+
+The reference's own adjoint (solver.py:290-329) is a subsampled continuous
+adjoint; ``seispie_b200.solver.b200.run_kernel`` reproduces that one.  This
+module is what makes finite-difference-exact gradients (and therefore
+autograd) possible.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from . import engine
+from ._lib import FWI_PSV, FWI_SH
+from .engine import COMP, NS, NV, DeviceModel, Grid, ShotBatch, adjoint_injection_lists, injection_lists
+
+
+def default_segment(nt: int, mode: int, nshots: int, grid: Grid, budget_bytes: float | None = None) -> int:
+    """Segment length K minimising checkpoint + segment memory
+    (nt/K * (NS+2NV) fields + K * 2NV fields), then shrunk to the budget."""
+    state = NS[mode] + 2 * NV[mode]
+    per_step = 2 * NV[mode]
+    k = max(1, int(round(math.sqrt(nt * state / per_step))))
+    if budget_bytes:
+        field = 4 * nshots * grid.nx * grid.pitch
+        while k > 1 and (math.ceil(nt / k) * state + k * per_step) * field > budget_bytes:
+            k = max(1, k // 2)
+    return min(k, nt)
+
+
+class ExactAdjoint:
+    """Forward with checkpoints, then exact backward, for one batch of shots."""
+
+    def __init__(self, model: DeviceModel, nt: int, src_id, isrc_of_shot, nshots: int, stf, rec_id,
+                 segment: int | None = None, tile: int = 0):
+        if model.mode not in (FWI_SH, FWI_PSV):
+            raise ValueError("the exact adjoint covers SH and P-SV")
+        self.model, self.nt, self.nshots = model, int(nt), int(nshots)
+        self.rec_id = np.asarray(rec_id, np.int32)
+        self.mode = model.mode
+        g = model.grid
+        self.K = segment or default_segment(self.nt, self.mode, self.nshots, g)
+        self.nseg = math.ceil(self.nt / self.K)
+        self.fwd = ShotBatch(model, self.nshots, self.nt, self.rec_id, tile=tile)
+        self.fdesc = self.fwd.desc(inj=injection_lists(self.nshots, src_id, isrc_of_shot), stf=stf)
+        dev = model.device
+        shape = (self.nshots, g.nx, g.pitch)
+        nstate = len(self.fwd.state_tensors())
+        self.ckpt = torch.empty((self.nseg, nstate) + shape, dtype=torch.float32, device=dev)
+        self.seg_v = [None, None, None]
+        self.seg_ds = [None, None, None]
+        for c in COMP[self.mode][: NV[self.mode]]:
+            self.seg_v[c] = torch.empty((self.K,) + shape, dtype=torch.float32, device=dev)
+            self.seg_ds[c] = torch.empty((self.K,) + shape, dtype=torch.float32, device=dev)
+
+    def forward(self) -> list:
+        """Run the forward, keeping a checkpoint every K steps; returns the
+        traces per component slot (None where absent), [nshots, nrec, nt]."""
+        b = self.fwd
+        b.clear()
+        for s in range(self.nseg):
+            for q, t in enumerate(b.state_tensors()):
+                self.ckpt[s, q].copy_(t)
+            n = min(self.K, self.nt - s * self.K)
+            b.run(self.fdesc, False, s * self.K, n)
+        return [b.traces(c).clone() if b.obs[c] is not None else None for c in range(3)]
+
+    def backward(self, g_traces: list) -> tuple:
+        """Exact gradients from trace gradients (per component slot, each
+        [nshots, nrec, nt] in forward time order).  Returns FP64
+        (dL/dlam, dL/dmu, dL/dbuo) on [nx, pitch] (dL/dlam is zero for SH)."""
+        gr = self.model.grid
+        dev = self.model.device
+        k = [torch.zeros((gr.nx, gr.pitch), dtype=torch.float64, device=dev) for _ in range(3)]
+        stf = [None, None, None]
+        for c in range(3):
+            if g_traces[c] is not None and self.fwd.obs[c] is not None:
+                stf[c] = g_traces[c].reshape(-1).to(torch.float32).contiguous()
+        adj = ShotBatch(self.model, self.nshots, self.nt, self.rec_id)
+        adj.clear()
+        inj = adjoint_injection_lists(self.nshots, self.rec_id) if len(self.rec_id) else None
+        adesc = adj.desc(inj=inj, stf=stf, record=False, kernels=k)
+        fwd = self.fwd
+        for s in reversed(range(self.nseg)):
+            s0, n = s * self.K, min(self.K, self.nt - s * self.K)
+            for q, t in enumerate(fwd.state_tensors()):
+                t.copy_(self.ckpt[s, q])
+            fwd.set_segment(self.fdesc, self.seg_v, self.seg_ds, s0, n)
+            fwd.run(self.fdesc, False, s0, n)
+            adj.set_segment(adesc, self.seg_v, self.seg_ds, s0, n)
+            adj.run_transposed(adesc, s0 + n, n)
+        fwd.set_segment(self.fdesc, [None] * 3, [None] * 3, 0, 0)
+        return tuple(k)
+
+
+def _pad(t: torch.Tensor, grid: Grid) -> torch.Tensor:
+    out = torch.zeros((grid.nx, grid.pitch), dtype=torch.float32, device=t.device)
+    out[:, : grid.nz] = t.reshape(grid.nx, grid.nz)
+    return out
+
+
+class Seismograms(torch.autograd.Function):
+    """(lam, mu, rho) -> receiver traces, differentiable.
+
+    Inputs are float32 CUDA tensors of shape [nx, nz] (the reference's cell
+    order).  ``setup`` is an :class:`AcquisitionSetup`.  Output: traces
+    [ncomp, nshots, nrec, nt] (SH: the y component; P-SV: x then z).
+    Gradients are the exact discrete adjoint (FP64 accumulation)."""
+
+    @staticmethod
+    def forward(ctx, lam, mu, rho, setup):
+        g = setup.grid
+        m = DeviceModel(g, setup.mode, setup.dt, lam.device)
+        m.lam.copy_(_pad(lam.detach(), g))
+        m.mu.copy_(_pad(mu.detach(), g))
+        m.rho.copy_(_pad(rho.detach(), g))
+        w, a, l, r, b, t = setup.absorb
+        lib = engine._lib.load()
+        engine.check(lib.fwi_set_bound(engine.ptr(m.bound), g.nx, g.nz, g.pitch, int(w), float(a), int(l), int(r),
+                                       int(b), int(t), engine.stream_handle(None)), "fwi_set_bound")
+        m.prepare()
+        ea = ExactAdjoint(m, setup.nt, setup.src_id, setup.isrc_of_shot, setup.nshots, setup.stf, setup.rec_id,
+                          segment=setup.segment)
+        tr = ea.forward()
+        comps = [c for c in range(3) if tr[c] is not None]
+        ctx.ea, ctx.comps, ctx.setup = ea, comps, setup
+        ctx.save_for_backward(rho)
+        return torch.stack([tr[c] for c in comps])
+
+    @staticmethod
+    def backward(ctx, grad):
+        (rho,) = ctx.saved_tensors
+        g = ctx.setup.grid
+        gt = [None, None, None]
+        for i, c in enumerate(ctx.comps):
+            gt[c] = grad[i]
+        k_lam, k_mu, k_buo = ctx.ea.backward(gt)
+        nz = g.nz
+        dlam = k_lam[:, :nz].reshape(g.nx, nz)
+        dmu = k_mu[:, :nz].reshape(g.nx, nz)
+        # buo = dt/rho rounded to float32 -> dL/drho = -dL/dbuo * dt / rho^2
+        drho = -k_buo[:, :nz].reshape(g.nx, nz) * ctx.setup.dt / rho.double() ** 2
+        ctx.ea = None
+        return dlam.float(), dmu.float(), drho.float(), None
+
+
+class AcquisitionSetup:
+    """Everything of a batched simulation except the model: grid, time axis,
+    sources (positions and Ricker parameters), receivers and sponge."""
+
+    def __init__(self, mode: str, grid: Grid, dt: float, nt: int, src: np.ndarray, rec: np.ndarray, absorb,
+                 combine_sources: bool = False, segment: int | None = None, device="cuda"):
+        from ._lib import MODES
+        self.mode = MODES[mode]
+        self.grid, self.dt, self.nt = grid, float(dt), int(nt)
+        self.absorb = absorb
+        self.src_id = engine.point_ids(np.asarray(src, np.float64), np.float32(grid.dx), np.float32(grid.dz), grid.nz)
+        self.rec_id = engine.point_ids(np.asarray(rec, np.float64), np.float32(grid.dx), np.float32(grid.dz), grid.nz)
+        self.nshots = 1 if combine_sources else len(self.src_id)
+        self.isrc_of_shot = (lambda s: -1) if combine_sources else (lambda s: s)
+        self.stf, self._par = engine.ricker_stf(np.asarray(src, np.float64), self.nt, self.dt, device)
+        self.segment = segment
+
+
+def hann_taper(nt: int, dt: float) -> np.ndarray:
+    """The misfit's time taper (waveform.py:11-21), float64."""
+    t_end = (nt - 1) * dt
+    tw = t_end / 10
+    t_min, t_max = tw, t_end - tw
+    w = np.ones(nt)
+    for it in range(nt):
+        t = it * dt
+        if t <= t_min:
+            w[it] = 0.5 + 0.5 * math.cos(math.pi * (t_min - t) / tw)
+        elif t >= t_max:
+            w[it] = 0.5 + 0.5 * math.cos(math.pi * (t_max - t) / tw)
+    return w
+
+
+def waveform_misfit(traces: torch.Tensor, data: torch.Tensor, dt: float) -> torch.Tensor:
+    """chi = sum taper^2 (syn - data)^2 in FP64 -- the objective whose negative
+    derivative is the reference's adjoint source 2 taper^2 (d - s)
+    (waveform.py:24-25)."""
+    w = torch.as_tensor(hann_taper(traces.shape[-1], dt), device=traces.device)
+    r = (traces.double() - data.double()) * w
+    return (r * r).sum()
+
+
+def vps_to_lame(vp: torch.Tensor, vs: torch.Tensor, rho: torch.Tensor):
+    """vps2lm (fd2d.py:21-33) in differentiable torch ops (vp > vs assumed)."""
+    return rho * (vp * vp - 2 * vs * vs), rho * vs * vs

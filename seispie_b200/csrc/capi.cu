@@ -35,6 +35,7 @@ int check_launch(const char *what) {
 int launch_step(const fwi_batch *b, int adjoint, int it, bool snap_u_next, int snap_u_slot, bool snap_v,
                 int snap_v_slot, cudaStream_t st);
 int launch_interaction(const fwi_batch *b, int isae, cudaStream_t st);
+int launch_adjoint_step(const fwi_batch *b, int it, cudaStream_t st);
 int launch_misfit(const float *data, const float *syn, float *adstf, double *misfit, double *partial, int nshots,
                   int nrec, int nt, double dt, cudaStream_t st);
 long long misfit_partials(int nrec, int nt);
@@ -209,6 +210,32 @@ int fwi_run(fwi_batch *b, int adjoint, int it0, int nsteps, void *stream) {
             rc = launch_interaction(b, it / sae, st);
             if (rc) return rc;
         }
+    }
+    return 0;
+}
+
+int fwi_run_transposed(fwi_batch *b, int it_hi, int nsteps, void *stream) {
+    int rc = check_batch(b, 0, 0, 0);
+    if (rc) return rc;
+    REQUIRE(b->mode == FWI_SH || b->mode == FWI_PSV, "fwi_run_transposed: SH or P-SV only");
+    REQUIRE(nsteps >= 0 && it_hi - nsteps >= 0 && it_hi <= b->nt, "fwi_run_transposed: steps [%d, %d) outside [0, %d)",
+            it_hi - nsteps, it_hi, b->nt);
+    REQUIRE(it_hi - nsteps >= b->seg0 && it_hi <= b->seg0 + b->nseg,
+            "fwi_run_transposed: steps [%d, %d) not stored in the segment [%d, %d)", it_hi - nsteps, it_hi, b->seg0,
+            b->seg0 + b->nseg);
+    const int cx = b->mode == FWI_SH ? 1 : 0;
+    REQUIRE(b->seg_v[cx] && b->seg_ds[cx] && (b->mode == FWI_SH || (b->seg_v[2] && b->seg_ds[2])),
+            "fwi_run_transposed: the segment stores seg_v / seg_ds are required");
+    REQUIRE(b->k_mu, "fwi_run_transposed: k_mu is required");
+    if (b->inj_ptr) {
+        REQUIRE(b->inj_cell && b->inj_row, "inj_cell and inj_row are required with inj_ptr");
+        REQUIRE(b->stf[cx] && (b->mode == FWI_SH || b->stf[2]), "fwi_run_transposed: trace gradients (stf) missing");
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    for (int it = it_hi - 1; it >= it_hi - nsteps; it--) {
+        rc = launch_adjoint_step(b, it, st);
+        if (rc) return rc;
+        b->cur ^= 1;
     }
     return 0;
 }

@@ -83,6 +83,8 @@ struct StepArgs {
     float *obs[3];
     float *snap_u[3];  // already offset to the slot, or NULL
     float *snap_v[3];
+    float *seg_v[3];   // per-step store of the new velocity (exact adjoint), slot-offset, or NULL
+    float *seg_ds[3];  // per-step store of the stress divergence incl. sources, or NULL
 };
 
 template <int MODE, int TX, int TZ>
@@ -284,7 +286,7 @@ __device__ __forceinline__ void stress_update(const StepArgs &a, const float *s0
 // snapshots, u into shared memory for the receivers.
 template <int MODE, int TX, int TZ>
 __device__ __forceinline__ void store_interior(const StepArgs &a, const Smem<MODE, TX, TZ> &sm, int ci, long long g,
-                                               const float (&v)[3]) {
+                                               const float (&v)[3], const float (&ds)[3]) {
 #pragma unroll
     for (int q = 0; q < Fields<MODE>::NV; q++) {
         const float u = sm.U[q * TX * TZ + ci] + v[q] * a.dt;
@@ -293,6 +295,8 @@ __device__ __forceinline__ void store_interior(const StepArgs &a, const Smem<MOD
         a.disp[q][g] = u;
         if (a.snap_u[q]) a.snap_u[q][g] = u;
         if (a.snap_v[q]) a.snap_v[q][g] = v[q];
+        if (a.seg_v[q]) a.seg_v[q][g] = v[q];
+        if (a.seg_ds[q]) a.seg_ds[q][g] = ds[q];
     }
 }
 
@@ -318,7 +322,7 @@ __device__ __forceinline__ void gather_receivers(const StepArgs &a, const Smem<M
 // shared memory).  Returns false for a cell outside the grid (v set to 0).
 template <int MODE, int TX, int TZ>
 __device__ __forceinline__ bool velocity_cell(const StepArgs &a, const Smem<MODE, TX, TZ> &sm, int x0, int z0, int rx,
-                                              int rz, bool has_inj, float (&v)[3]) {
+                                              int rz, bool has_inj, float (&v)[3], float (&ds)[3]) {
     using T = Tile<MODE, TX, TZ>;
     constexpr int SX = T::SX, SZ = T::SZ, VX = T::VX;
     const int gx = x0 - 1 + rx, gz = z0 - 1 + rz;
@@ -342,7 +346,6 @@ __device__ __forceinline__ bool velocity_cell(const StepArgs &a, const Smem<MODE
         return cz1 * (s[0] - s[-1]) - cz2 * (s[1] - s[-2]);
     };
     auto center = [&](int f) -> float { return s0[f * SX * SZ]; };
-    float ds[3];
     divergence<MODE>(dxm, dzm, center, ds);
     velocity_update<MODE, TX, TZ>(sm, rx, rz, ds, has_inj, v);
     return true;
@@ -366,8 +369,8 @@ __device__ __forceinline__ void velocity_halo(const StepArgs &a, const Smem<MODE
             rx = 1 + c2 / 3;
             rz = k3 == 0 ? 0 : TZ + k3;
         }
-        float v[3];
-        velocity_cell<MODE, TX, TZ>(a, sm, x0, z0, rx, rz, has_inj, v);
+        float v[3], ds[3];
+        velocity_cell<MODE, TX, TZ>(a, sm, x0, z0, rx, rz, has_inj, v, ds);
     }
 }
 
@@ -386,9 +389,9 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 2) step_kerne
 
     for (int c = threadIdx.x; c < TX * TZ; c += kThreads) {
         const int ix = c / TZ, iz = c - ix * TZ;
-        float v[3];
-        if (velocity_cell<MODE, TX, TZ>(a, sm, x0, z0, ix + 1, iz + 1, has_inj, v))
-            store_interior<MODE, TX, TZ>(a, sm, c, soff + (long long)(x0 + ix) * pitch + (z0 + iz), v);
+        float v[3], ds[3];
+        if (velocity_cell<MODE, TX, TZ>(a, sm, x0, z0, ix + 1, iz + 1, has_inj, v, ds))
+            store_interior<MODE, TX, TZ>(a, sm, c, soff + (long long)(x0 + ix) * pitch + (z0 + iz), v, ds);
     }
     velocity_halo<MODE, TX, TZ>(a, sm, x0, z0, has_inj);
     __syncthreads();
@@ -473,7 +476,7 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 3) step_kerne
             float ds[3], v[3];
             divergence<MODE>(dxm, dzm, center, ds);
             velocity_update<MODE, TX, TZ>(sm, ix + 1, lane + 1, ds, has_inj, v);
-            store_interior<MODE, TX, TZ>(a, sm, ix * TZ + lane, soff + (long long)gx * pitch + gz, v);
+            store_interior<MODE, TX, TZ>(a, sm, ix * TZ + lane, soff + (long long)gx * pitch + gz, v, ds);
         }
     }
     velocity_halo<MODE, TX, TZ>(a, sm, x0, z0, has_inj);
@@ -509,6 +512,380 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 3) step_kerne
                                         soff + (long long)gx * pitch + gz, dxp, dzp);
         }
     }
+}
+
+// ------------------------------------------------ exact discrete adjoint
+//
+// The forward step above is linear in the state.  For SH / P-SV it reads
+//   d  = D- sig + f            (stress divergence plus sources)
+//   v' = B (v + b d)           (b = dt/rho, B = sponge)
+//   u' = u + dt v'
+//   sig' = sig + dt S(D+ v')   (S: lam/mu stress-strain law)
+// Its exact transpose, run backwards in time on the adjoint state
+// (sig~, v~, u~), is one launch of adjoint_kernel per step:
+//   u~  += P^T g               (g = dL/d(trace) of this step, at receivers)
+//   a    = v~ + dt u~ + (D+)^T (dt S^T sig~)
+//   v~'  = B a
+//   sig~' = sig~ + (D-)^T (b v~')
+// with (D+)^T and (D-)^T the transposes of the reference's masked stencils
+// (solver.py:22-51) -- boundary masks included, so the adjoint is exact to
+// rounding.  grad_kernel then adds this step's terms of
+//   dL/dlam = sum dt (sxx~+szz~)(exx+ezz),
+//   dL/dmu  = sum dt (2 sxx~ exx + 2 szz~ ezz + sxz~ (exz+ezx))  [SH: dt (sxy~ exy + szy~ ezy)]
+//   dL/db   = sum v~' . d
+// from the forward v' and d stored per step by a recomputed forward segment.
+
+struct AdjArgs {
+    int nx, nz, pitch, nt, it;
+    FastDiv divnz;
+    float cx1, cx2, cz1, cz2, dt;
+    const float *sig_in[3];
+    float *sig_out[3];
+    const float *vel_in[2];
+    float *vel_out[2];
+    float *disp[2];
+    const float *buo, *bound, *lam, *mu;
+    const int *inj_ptr, *inj_cell, *inj_row;
+    const float *g[2];  // trace gradients in forward time order, injected into u~
+};
+
+template <int MODE, int TX, int TZ>
+struct AdjTile {
+    using F = Fields<MODE>;
+    static constexpr int SX = TX + 6, SZ = TZ + 8, VX = TX + 3, RVZ = TZ + 3;
+    static constexpr int NL = MODE == FWI_SH ? 1 : 2;   // stiffness fields staged with halo
+    static constexpr int NTT = MODE == FWI_SH ? 2 : 3;  // dt S^T sig~ fields
+    static constexpr int FS = (SX * SZ + 3) / 4 * 4, FV = (VX * SZ + 3) / 4 * 4;
+    static constexpr int S_SZ = (F::NS + NL + NTT) * FS;
+    static constexpr int V_SZ = (2 * F::NV + 2) * FV;
+    static constexpr int J_SZ = F::NINJ * VX * RVZ;
+    static constexpr int LIST = kThreads * (1 + F::NINJ) + 8;
+    static constexpr size_t bytes = sizeof(float) * (size_t)(S_SZ + V_SZ + J_SZ + LIST);
+};
+
+// Stage NF fields (field stride FSTR floats) of a ROWS x COLS window.
+template <int NF, int ROWS, int COLS, int FSTR>
+__device__ __forceinline__ void stage_strided(float *dst, const float *const *src, long long off, int gx0, int gz0,
+                                              int nx, int pitch, int tid) {
+    constexpr int C4 = COLS / 4, PER = ROWS * C4;
+    for (int q = tid; q < PER; q += kThreads) {
+        const int r = q / C4, c = q - r * C4;
+        const int gx = gx0 + r, gz = gz0 + 4 * c;
+        const bool ok = gx >= 0 && gx < nx && gz >= 0 && gz < pitch;
+        const long long o = ok ? off + (long long)gx * pitch + gz : 0;
+#pragma unroll
+        for (int f = 0; f < NF; f++) cp_async16(dst + f * FSTR + r * COLS + 4 * c, src[f] + o, ok ? 16 : 0);
+    }
+}
+
+// Entries of this shot at cells of the computed region, summed per cell in
+// entry order into J (NINJ components, VX x RVZ cells).  Returns whether any
+// entry falls in the tile.
+template <int NINJ, int VX, int RVZ>
+__device__ __forceinline__ bool scatter_entries(const int *inj_ptr, const int *inj_cell, const int *inj_row,
+                                                const float *const *val_src, int nt, int it, const FastDiv &divnz,
+                                                int nz, int x0, int z0, int shot, float *J, int *sLoc, float *sVal,
+                                                int *sWarp) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    bool has = false;
+    if (!inj_ptr) return false;
+    const int p0 = inj_ptr[shot], p1 = inj_ptr[shot + 1];
+    for (int base = p0; base < p1; base += kThreads) {
+        const int e = base + tid;
+        int loc = -1;
+        float val[NINJ];
+        if (e < p1) {
+            const int k = inj_cell[e];
+            const int gx = fdiv(k, divnz), gz = k - gx * nz;
+            const int rx = gx - (x0 - 1), rz = gz - (z0 - 1);
+            if (rx >= 0 && rx < VX && rz >= 0 && rz < RVZ) {
+                loc = rx * RVZ + rz;
+                const long long src = (long long)inj_row[e] * nt + it;
+#pragma unroll
+                for (int c = 0; c < NINJ; c++) val[c] = val_src[c][src];
+            }
+        }
+        const int n_in = __syncthreads_count(loc >= 0);
+        if (n_in == 0) continue;
+        if (!has) {
+            for (int q = tid; q < NINJ * VX * RVZ; q += kThreads) J[q] = 0.f;
+            has = true;
+        }
+        const unsigned ball = __ballot_sync(0xffffffffu, loc >= 0);
+        if (lane == 0) sWarp[warp] = __popc(ball);
+        __syncthreads();
+        if (loc >= 0) {
+            int pos = __popc(ball & ((1u << lane) - 1u));
+            for (int w = 0; w < warp; w++) pos += sWarp[w];
+            sLoc[pos] = loc;
+#pragma unroll
+            for (int c = 0; c < NINJ; c++) sVal[c * kThreads + pos] = val[c];
+        }
+        __syncthreads();
+        if (tid == 0) {
+            for (int q = 0; q < n_in; q++) {
+#pragma unroll
+                for (int c = 0; c < NINJ; c++) J[c * VX * RVZ + sLoc[q]] += sVal[c * kThreads + q];
+            }
+        }
+        __syncthreads();
+    }
+    return has;
+}
+
+template <int MODE, int TX, int TZ>
+__global__ void __launch_bounds__(kThreads, 2) adjoint_kernel(const AdjArgs a) {
+    using T = AdjTile<MODE, TX, TZ>;
+    using F = Fields<MODE>;
+    constexpr int SX = T::SX, SZ = T::SZ, VX = T::VX, RVZ = T::RVZ, FS = T::FS, FV = T::FV;
+    constexpr int NS = F::NS, NV = F::NV, NL = T::NL;
+    extern __shared__ __align__(16) float smem[];
+    float *sSig = smem, *sL = sSig + NS * FS, *sT = sL + NL * FS;
+    float *sV = sT + T::NTT * FS, *sU = sV + NV * FV, *sB = sU + NV * FV;
+    float *sJ = sB + 2 * FV;
+    int *sLoc = reinterpret_cast<int *>(sJ + T::J_SZ);
+    float *sVal = reinterpret_cast<float *>(sLoc + kThreads);
+    int *sWarp = reinterpret_cast<int *>(sVal + F::NINJ * kThreads);
+
+    const int tid = threadIdx.x;
+    const int z0 = blockIdx.x * TZ, x0 = blockIdx.y * TX, shot = blockIdx.z;
+    const int nx = a.nx, nz = a.nz, pitch = a.pitch;
+    const long long soff = (long long)shot * nx * pitch;
+    const float *lm[2] = {MODE == FWI_SH ? a.mu : a.lam, a.mu};
+    const float *bb[2] = {a.buo, a.bound};
+    stage_strided<NS, SX, SZ, FS>(sSig, a.sig_in, soff, x0 - 3, z0 - 4, nx, pitch, tid);
+    stage_strided<NL, SX, SZ, FS>(sL, lm, 0, x0 - 3, z0 - 4, nx, pitch, tid);
+    stage_strided<NV, VX, SZ, FV>(sV, a.vel_in, soff, x0 - 1, z0 - 4, nx, pitch, tid);
+    stage_strided<NV, VX, SZ, FV>(sU, a.disp, soff, x0 - 1, z0 - 4, nx, pitch, tid);
+    stage_strided<2, VX, SZ, FV>(sB, bb, 0, x0 - 1, z0 - 4, nx, pitch, tid);
+    cp_async_commit();
+    const bool has_inj = scatter_entries<F::NINJ, VX, RVZ>(a.inj_ptr, a.inj_cell, a.inj_row, a.g, a.nt, a.it,
+                                                           a.divnz, nz, x0, z0, shot, sJ, sLoc, sVal, sWarp);
+    cp_async_wait_all();
+    __syncthreads();
+
+    const float dt = a.dt, cx1 = a.cx1, cx2 = a.cx2, cz1 = a.cz1, cz2 = a.cz2;
+    // t = dt S^T sig~ over the whole stress region (zero outside the grid)
+    for (int c = tid; c < SX * SZ; c += kThreads) {
+        if (MODE == FWI_SH) {
+            const float m = sL[c];
+            sT[c] = dt * (m * sSig[c]);
+            sT[FS + c] = dt * (m * sSig[FS + c]);
+        } else {
+            const float l = sL[c], m = sL[FS + c], l2m = l + 2.f * m;
+            const float sxx = sSig[c], szz = sSig[FS + c], sxz = sSig[2 * FS + c];
+            sT[c] = dt * (l2m * sxx + l * szz);
+            sT[FS + c] = dt * (l * sxx + l2m * szz);
+            sT[2 * FS + c] = dt * (m * sxz);
+        }
+    }
+    __syncthreads();
+
+    // velocity-like half on the computed region (rows x0-1..x0+TX+1, columns z0-1..z0+TZ+1)
+    auto mxp = [&](int k) -> float { return (k >= 1 && k < nx - 2) ? 1.f : 0.f; };
+    auto mzp = [&](int k) -> float { return (k >= 1 && k < nz - 2) ? 1.f : 0.f; };
+    for (int c = tid; c < VX * RVZ; c += kThreads) {
+        const int rx = c / RVZ, rz = c - rx * RVZ;
+        const int gx = x0 - 1 + rx, gz = z0 - 1 + rz;
+        const int vi = rx * SZ + rz + 3, si = (rx + 2) * SZ + rz + 3;
+        if (gx < 0 || gx >= nx || gz < 0 || gz >= nz) {
+#pragma unroll
+            for (int q = 0; q < NV; q++) sV[q * FV + vi] = 0.f;
+            continue;
+        }
+        // (D+)^T along x and z of field f of t
+        auto dxpT = [&](int f) -> float {
+            const float *t = sT + f * FS + si;
+            return cx1 * (t[-SZ] * mxp(gx - 1) - t[0] * mxp(gx)) - cx2 * (t[-2 * SZ] * mxp(gx - 2) - t[SZ] * mxp(gx + 1));
+        };
+        auto dzpT = [&](int f) -> float {
+            const float *t = sT + f * FS + si;
+            return cz1 * (t[-1] * mzp(gz - 1) - t[0] * mzp(gz)) - cz2 * (t[-2] * mzp(gz - 2) - t[1] * mzp(gz + 1));
+        };
+        float acc[2];
+        if (MODE == FWI_SH) {
+            acc[0] = dxpT(0) + dzpT(1);
+        } else {
+            acc[0] = dxpT(0) + dzpT(2);
+            acc[1] = dxpT(2) + dzpT(1);
+        }
+        const bool interior = rx >= 1 && rx <= TX && rz >= 1 && rz <= TZ;
+        const long long g = soff + (long long)gx * pitch + gz;
+        const float bnd = sB[FV + vi], buo = sB[vi];
+#pragma unroll
+        for (int q = 0; q < NV; q++) {
+            float uu = sU[q * FV + vi];
+            if (has_inj) uu += sJ[q * VX * RVZ + rx * RVZ + rz];
+            const float vn = bnd * ((sV[q * FV + vi] + dt * uu) + acc[q]);
+            sV[q * FV + vi] = buo * vn;  // b v~' for the stress-like half
+            if (interior) {
+                a.vel_out[q][g] = vn;
+                a.disp[q][g] = uu;
+            }
+        }
+    }
+    __syncthreads();
+
+    // stress-like half on the interior: sig~' = sig~ + (D-)^T (b v~')
+    auto mxm = [&](int k) -> float { return (k >= 2 && k < nx - 2) ? 1.f : 0.f; };
+    auto mzm = [&](int k) -> float { return (k >= 2 && k < nz - 2) ? 1.f : 0.f; };
+    for (int c = tid; c < TX * TZ; c += kThreads) {
+        const int ix = c / TZ, iz = c - ix * TZ;
+        const int gx = x0 + ix, gz = z0 + iz;
+        if (gx >= nx || gz >= nz) continue;
+        const int vi = (ix + 1) * SZ + iz + 4, si = (ix + 3) * SZ + iz + 4;
+        auto dxmT = [&](int q) -> float {
+            const float *w = sV + q * FV + vi;
+            return cx1 * (w[0] * mxm(gx) - w[SZ] * mxm(gx + 1)) - cx2 * (w[-SZ] * mxm(gx - 1) - w[2 * SZ] * mxm(gx + 2));
+        };
+        auto dzmT = [&](int q) -> float {
+            const float *w = sV + q * FV + vi;
+            return cz1 * (w[0] * mzm(gz) - w[1] * mzm(gz + 1)) - cz2 * (w[-1] * mzm(gz - 1) - w[2] * mzm(gz + 2));
+        };
+        const long long g = soff + (long long)gx * pitch + gz;
+        if (MODE == FWI_SH) {
+            a.sig_out[0][g] = sSig[si] + dxmT(0);
+            a.sig_out[1][g] = sSig[FS + si] + dzmT(0);
+        } else {
+            a.sig_out[0][g] = sSig[si] + dxmT(0);
+            a.sig_out[1][g] = sSig[FS + si] + dzmT(1);
+            a.sig_out[2][g] = sSig[2 * FS + si] + (dzmT(0) + dxmT(1));
+        }
+    }
+}
+
+// This step's gradient terms, all shots of the batch summed per cell in shot
+// order into FP64 accumulators ([nx][pitch]).  sig_adj: sig~ before the
+// transposed step (adjoint of sig(it+1)); vel_adj: v~ after it (= B a);
+// vf: forward v(it+1); dsf: forward divergence of step it.
+struct AdjPtrs {
+    const float *sig_adj[3], *vel_adj[2], *vf[2], *dsf[2];
+};
+
+template <int MODE>
+__global__ void grad_kernel(const AdjPtrs p, double *k_lam, double *k_mu, double *k_buo, int nx, int nz, int pitch,
+                            int nshots, float cx1, float cx2, float cz1, float cz2, double dt) {
+    const float *const *sig_adj = p.sig_adj;
+    const float *const *vel_adj = p.vel_adj;
+    const float *const *vf = p.vf;
+    const float *const *dsf = p.dsf;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+    if (j >= nz) return;
+    const bool okx = i >= 1 && i < nx - 2, okz = j >= 1 && j < nz - 2;
+    const long long o = (long long)i * pitch + j, field = (long long)nx * pitch;
+    double al = 0.0, am = 0.0, ab = 0.0;
+    for (int s = 0; s < nshots; s++) {
+        const long long g = s * field + o;
+        auto dxp = [&](const float *v) -> float {
+            return okx ? cx1 * (v[g + pitch] - v[g]) - cx2 * (v[g + 2 * pitch] - v[g - pitch]) : 0.f;
+        };
+        auto dzp = [&](const float *v) -> float {
+            return okz ? cz1 * (v[g + 1] - v[g]) - cz2 * (v[g + 2] - v[g - 1]) : 0.f;
+        };
+        if (MODE == FWI_SH) {
+            am += ((double)sig_adj[0][g] * dxp(vf[0]) + (double)sig_adj[1][g] * dzp(vf[0])) * dt;
+            ab += (double)vel_adj[0][g] * dsf[0][g];
+        } else {
+            const double exx = dxp(vf[0]), exz = dzp(vf[0]), ezx = dxp(vf[1]), ezz = dzp(vf[1]);
+            const double sxx = sig_adj[0][g], szz = sig_adj[1][g], sxz = sig_adj[2][g];
+            al += (sxx + szz) * (exx + ezz) * dt;
+            am += (2.0 * (sxx * exx + szz * ezz) + sxz * (exz + ezx)) * dt;
+            ab += (double)vel_adj[0][g] * dsf[0][g] + (double)vel_adj[1][g] * dsf[1][g];
+        }
+    }
+    if (k_lam && MODE != FWI_SH) k_lam[o] += al;
+    if (k_mu) k_mu[o] += am;
+    if (k_buo) k_buo[o] += ab;
+}
+
+// One transposed step (forward step `it`, adjoint state it+1 -> it) and its
+// gradient terms.
+int launch_adjoint_step(const fwi_batch *b, int it, cudaStream_t st) {
+    AdjArgs a;
+    a.nx = b->nx;
+    a.nz = b->nz;
+    a.pitch = b->pitch;
+    a.nt = b->nt;
+    a.it = it;
+    a.divnz = make_fastdiv(b->nz);
+    a.cx1 = (float)(9.0 / (8.0 * (double)b->dx));
+    a.cx2 = (float)(1.0 / (24.0 * (double)b->dx));
+    a.cz1 = (float)(9.0 / (8.0 * (double)b->dz));
+    a.cz2 = (float)(1.0 / (24.0 * (double)b->dz));
+    a.dt = (float)b->dt;
+    const int cur = b->cur, nxt = 1 - b->cur;
+    const int ns = b->mode == FWI_SH ? 2 : 3, nv = b->mode == FWI_SH ? 1 : 2;
+    for (int f = 0; f < 3; f++) {
+        a.sig_in[f] = f < ns ? b->sig[cur][f] : nullptr;
+        a.sig_out[f] = f < ns ? b->sig[nxt][f] : nullptr;
+    }
+    for (int q = 0; q < 2; q++) {
+        a.vel_in[q] = q < nv ? b->vel[cur][q] : nullptr;
+        a.vel_out[q] = q < nv ? b->vel[nxt][q] : nullptr;
+        a.disp[q] = q < nv ? b->disp[q] : nullptr;
+    }
+    a.buo = b->buo;
+    a.bound = b->bound;
+    a.lam = b->lam;
+    a.mu = b->mu;
+    a.inj_ptr = b->inj_ptr;
+    a.inj_cell = b->inj_cell;
+    a.inj_row = b->inj_row;
+    if (b->mode == FWI_SH) {
+        a.g[0] = b->stf[1];
+        a.g[1] = nullptr;
+    } else {
+        a.g[0] = b->stf[0];
+        a.g[1] = b->stf[2];
+    }
+    constexpr int TX = 32, TZ = 32;
+    dim3 grid((b->nz + TZ - 1) / TZ, (b->nx + TX - 1) / TX, b->nshots);
+    if (b->mode == FWI_SH) {
+        using T = AdjTile<FWI_SH, TX, TZ>;
+        static bool set = false;
+        if (!set) {
+            cudaError_t e = cudaFuncSetAttribute(adjoint_kernel<FWI_SH, TX, TZ>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::bytes);
+            if (e != cudaSuccess) return set_error(FWI_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+            set = true;
+        }
+        adjoint_kernel<FWI_SH, TX, TZ><<<grid, kThreads, T::bytes, st>>>(a);
+    } else {
+        using T = AdjTile<FWI_PSV, TX, TZ>;
+        static bool set = false;
+        if (!set) {
+            cudaError_t e = cudaFuncSetAttribute(adjoint_kernel<FWI_PSV, TX, TZ>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::bytes);
+            if (e != cudaSuccess) return set_error(FWI_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+            set = true;
+        }
+        adjoint_kernel<FWI_PSV, TX, TZ><<<grid, kThreads, T::bytes, st>>>(a);
+    }
+    int rc = check_launch("adjoint_kernel");
+    if (rc) return rc;
+    // gradient terms of this step
+    const long long field = (long long)b->nshots * b->nx * b->pitch;
+    const int slot = it - b->seg0;
+    const float *sa[3] = {a.sig_in[0], a.sig_in[1], a.sig_in[2]};
+    const float *va[2] = {a.vel_out[0], a.vel_out[1]};
+    const int cx = b->mode == FWI_SH ? 1 : 0, czs = b->mode == FWI_SH ? 1 : 2;
+    const float *vf[2] = {b->seg_v[cx] + slot * field, nv > 1 ? b->seg_v[czs] + slot * field : nullptr};
+    const float *df[2] = {b->seg_ds[cx] + slot * field, nv > 1 ? b->seg_ds[czs] + slot * field : nullptr};
+    dim3 g2((b->nz + 127) / 128, b->nx);
+    AdjPtrs ptrs;
+    for (int f = 0; f < 3; f++) ptrs.sig_adj[f] = sa[f];
+    for (int q = 0; q < 2; q++) {
+        ptrs.vel_adj[q] = va[q];
+        ptrs.vf[q] = vf[q];
+        ptrs.dsf[q] = df[q];
+    }
+    if (b->mode == FWI_SH)
+        grad_kernel<FWI_SH><<<g2, 128, 0, st>>>(ptrs, nullptr, b->k_mu, b->k_rho, b->nx, b->nz, b->pitch, b->nshots,
+                                               a.cx1, a.cx2, a.cz1, a.cz2, b->dt);
+    else
+        grad_kernel<FWI_PSV><<<g2, 128, 0, st>>>(ptrs, b->k_lam, b->k_mu, b->k_rho, b->nx, b->nz, b->pitch,
+                                                b->nshots, a.cx1, a.cx2, a.cz1, a.cz2, b->dt);
+    return check_launch("grad_kernel");
 }
 
 // ------------------------------------------------------------- launching
@@ -632,6 +1009,9 @@ int launch_step(const fwi_batch *b, int adjoint, int it, bool snap_u_next, int s
                                                                           : nullptr;
         a.snap_v[q] = (on && !adjoint && snap_v && b->snap_v[slot]) ? b->snap_v[slot] + snap_v_slot * field
                                                                      : nullptr;
+        const bool seg = on && !adjoint && it - b->seg0 >= 0 && it - b->seg0 < b->nseg;
+        a.seg_v[q] = (seg && b->seg_v[slot]) ? b->seg_v[slot] + (long long)(it - b->seg0) * field : nullptr;
+        a.seg_ds[q] = (seg && b->seg_ds[slot]) ? b->seg_ds[slot] + (long long)(it - b->seg0) * field : nullptr;
     }
     if (b->mode == FWI_SH) {
         a.stf[0] = b->stf[1];

@@ -214,6 +214,24 @@ class ShotBatch:
         b.k_lam, b.k_mu, b.k_rho = (ptr(k) for k in kernels)
         return b
 
+    def set_segment(self, b: FwiBatch, seg_v, seg_ds, seg0: int, nseg: int) -> FwiBatch:
+        """Point a descriptor at per-step segment stores (exact adjoint)."""
+        for c in range(3):
+            b.seg_v[c] = ptr(seg_v[c])
+            b.seg_ds[c] = ptr(seg_ds[c])
+        b.seg0, b.nseg = int(seg0), int(nseg)
+        return b
+
+    def run_transposed(self, desc: FwiBatch, it_hi: int, nsteps: int) -> None:
+        desc.cur = self.cur
+        check(_lib.load().fwi_run_transposed(ctypes.byref(desc), int(it_hi), int(nsteps),
+                                             stream_handle(self.stream)), "fwi_run_transposed")
+        self.cur = desc.cur
+
+    def state_tensors(self):
+        """Current wavefield tensors (stress, velocity, displacement)."""
+        return self.sig[self.cur] + self.vel[self.cur] + self.disp
+
     def clear(self) -> None:
         """Zero the wavefields (clear_wavefields, fd2d.py:318-341)."""
         with torch.cuda.stream(self.stream) if self.stream is not None else _null():
