@@ -192,6 +192,20 @@ int fwi_misfit(const float *data, const float *syn, float *adstf, double *misfit
                double *partial, int nshots, int nrec, int nt, double dt, void *stream);
 long long fwi_misfit_partials(int nrec, int nt);
 
+/* Optimizer vector kernels (float32 vectors of n elements, FP64 arithmetic).
+ * fwi_dot: *out = sum x[i]*y[i] in FP64, deterministic; partial is caller
+ *   scratch of fwi_reduce_partials() doubles.  Replaces np.dot of
+ *   lbfgs.py:37-45, cg.py:20-29, bracket.py:23-30,49-50.
+ * fwi_absmax: *out = max |x[i]| (partial: fwi_reduce_partials() floats).
+ *   Replaces np.amax(abs(.)), bracket.py:48-49.
+ * fwi_axpby: out = a*x + b*y evaluated in FP64, stored float32 (y may be
+ *   NULL); out may alias x or y.  Replaces the float64-scalar updates
+ *   q -= al*y, q += s*(al-be), m + alpha*p (lbfgs.py:40-46, bracket.py:59). */
+long long fwi_reduce_partials(void);
+int fwi_dot(const float *x, const float *y, long long n, double *out, double *partial, void *stream);
+int fwi_absmax(const float *x, long long n, float *out, float *partial, void *stream);
+int fwi_axpby(float *out, double a, const float *x, double b, const float *y, long long n, void *stream);
+
 /* Capacity, in FP64 partial sums, of the fixed scratch of fwi_misfit_noalloc
  * (1 MiB): nshots * fwi_misfit_partials(nrec, nt) must not exceed it. */
 #define FWI_MISFIT_NOALLOC_MAX_PARTIALS (1 << 17)

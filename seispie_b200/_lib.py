@@ -76,6 +76,10 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
         "fwi_misfit": ([_vp, _vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _vp],
                        ctypes.c_int),
         "fwi_misfit_partials": ([ctypes.c_int, ctypes.c_int], ctypes.c_longlong),
+        "fwi_reduce_partials": ([], ctypes.c_longlong),
+        "fwi_dot": ([_vp, _vp, ctypes.c_longlong, _vp, _vp, _vp], ctypes.c_int),
+        "fwi_absmax": ([_vp, ctypes.c_longlong, _vp, _vp, _vp], ctypes.c_int),
+        "fwi_axpby": ([_vp, ctypes.c_double, _vp, ctypes.c_double, _vp, ctypes.c_longlong, _vp], ctypes.c_int),
         "fwi_misfit_noalloc": ([_vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _vp],
                                ctypes.c_int),
         "fwi_smooth": ([_vp, ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp],

@@ -466,6 +466,22 @@ class b200:
         self.stream.synchronize()
         return out_k, misfit, out_m
 
+    def compute_gradient_device(self):
+        """compute_gradient without leaving the device: (smoothed k_mu, misfit,
+        mu) as float32 CUDA vectors of npt (the GPU optimizers' entry)."""
+        misfit, kernel, model = self.run_kernel(1)
+        with self._ctx():
+            g = kernel.tensor.reshape(-1).clone()
+            m = model._flat().clone()
+        self.stream.synchronize()
+        return g, misfit, m
+
+    def update_model_device(self, mu: torch.Tensor):
+        """update_model from a float32 CUDA vector of npt."""
+        torch.cuda.current_stream().synchronize()
+        with self._ctx():
+            self.model.mu[:, : self.nz].copy_(mu.reshape(self.nx, self.nz))
+
     def smooth(self, data):
         """fd2d.py:349-352: Gaussian smoothing of a device field (FP64
         [nx, pitch] tensor, or a DeviceArray); returns a float32 DeviceArray."""

@@ -268,7 +268,68 @@ def case_example_geometry():
     print("%-16s %dx%d  %.1fs" % ("example_geometry", s.nx, s.nz, time.time() - t0))
 
 
-CASES = dict(sh_fwd=case_sh_fwd, psv_fwd=case_psv_fwd, spin_fwd=case_spin_fwd, sh_grad=case_sh_grad,
+def case_optimize():
+    """The reference's L-BFGS (with its backtracking line search) and CG
+    (with the bracketing line search) on a weighted quadratic misfit, driven
+    by the loop of optimize/base.py:28-50 with a stand-in solver; records every
+    gradient, direction, line-search status and trial model."""
+    from seispie.optimize.cg import cg
+    from seispie.optimize.lbfgs import lbfgs
+    rng = np.random.default_rng(16)
+    n = 96
+    w = rng.uniform(0.5, 4.0, n)
+    mt = rng.uniform(2.0, 3.0, n)
+    m0 = (mt + rng.uniform(-0.4, 0.4, n)).astype("float32")
+
+    class Solver:
+        def __init__(self):
+            self.m = m0.copy()
+            self.trials = []
+
+        def update_model(self, m):
+            self.m = np.asarray(m, dtype="float32").copy()
+            self.trials.append(self.m.copy())
+
+        def compute_misfit(self):
+            return float(np.sum(w * (self.m.astype("float64") - mt) ** 2))
+
+        def gradient(self):
+            return (2 * w * (self.m.astype("float64") - mt)).astype("float32")
+
+    class Workflow:
+        pass
+
+    out = dict(w=w, mt=mt, m0=m0)
+    for name, cls in (("lbfgs", lbfgs), ("cg", cg)):
+        s = Solver()
+        wf = Workflow()
+        wf.solver = s
+        opt = cls()
+        opt.config = dict(niter="6", ls_step="10", ls_step_max="0.5", ls_step_init="0.05", ls_thresh="1.2",
+                          lbfgs_mem="3")
+        opt.mpi = None
+        opt.setup(wf)
+        gs, ps, st, ms, mis, ntr = [], [], [], [], [], []
+        for i in range(6):
+            opt.g_new, misfit, opt.m_new = s.gradient(), s.compute_misfit(), s.m.copy()
+            opt.p_new = opt.compute_direction()
+            opt.m_old, opt.p_old, opt.g_old = opt.m_new, opt.p_new, opt.g_new
+            status = opt.line_search(misfit)
+            gs.append(opt.g_new)
+            ps.append(np.asarray(opt.p_new, dtype="float32"))
+            st.append(status)
+            ms.append(s.m.copy())
+            mis.append(misfit)
+            ntr.append(len(s.trials))
+            if status < 0:
+                break
+        out.update({name + "_g": np.stack(gs), name + "_p": np.stack(ps), name + "_status": np.array(st),
+                    name + "_m": np.stack(ms), name + "_misfit": np.array(mis), name + "_ntrials": np.array(ntr)})
+    np.savez_compressed(os.path.join(OUT, "optimize.npz"), **out)
+    print("%-16s lbfgs status %s, cg status %s" % ("optimize", out["lbfgs_status"], out["cg_status"]))
+
+
+CASES = dict(optimize=case_optimize, sh_fwd=case_sh_fwd, psv_fwd=case_psv_fwd, spin_fwd=case_spin_fwd, sh_grad=case_sh_grad,
              misfit_smooth=case_misfit_smooth, example_geometry=case_example_geometry)
 
 if __name__ == "__main__":
