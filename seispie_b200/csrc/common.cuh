@@ -1,5 +1,6 @@
 // Shared device helpers for libseispie_b200 (sm_100a).
 #pragma once
+#include <cuda.h>  // CUtensorMap (the driver entry point is fetched at run time)
 #include <cuda_runtime.h>
 #include <stdint.h>
 

@@ -94,14 +94,18 @@ struct Tile {
     // x0+TX+1 reaches x0+TX+2), columns z0-4 .. z0+TZ+3
     static constexpr int SX = TX + 6, SZ = TZ + 8;
     static constexpr int VX = TX + 3, RVZ = TZ + 3;  // velocity rows / computed columns
-    static constexpr int S_SZ = F::NS * SX * SZ;
-    static constexpr int V_SZ = F::NV * VX * SZ;
-    static constexpr int P_SZ = F::NVP * VX * SZ;
+    // per-field strides padded to 128 bytes (TMA destinations must be aligned)
+    static constexpr int FS = (SX * SZ + 31) / 32 * 32, FV = (VX * SZ + 31) / 32 * 32;
+    static constexpr int S_SZ = F::NS * FS;
+    static constexpr int V_SZ = F::NV * FV;
+    static constexpr int P_SZ = F::NVP * FV;
     static constexpr int U_SZ = F::NV * TX * TZ;
     static constexpr int I_SZ = F::NIP * TX * TZ;
     static constexpr int J_SZ = F::NINJ * VX * RVZ;
     static constexpr int LIST = kThreads * (1 + F::NINJ) + 8;  // compacted injection entries + warp counts
-    static constexpr size_t bytes = sizeof(float) * (size_t)(S_SZ + V_SZ + P_SZ + U_SZ + I_SZ + J_SZ + LIST);
+    // mbarrier of the TMA variant after the list, 8-byte aligned
+    static constexpr int BAR_OFF = (S_SZ + V_SZ + P_SZ + U_SZ + I_SZ + J_SZ + LIST + 1) / 2 * 2;
+    static constexpr size_t bytes = sizeof(float) * (size_t)(BAR_OFF + 2);
     static_assert(TZ % 4 == 0, "TZ must be a multiple of 4");
 };
 
@@ -124,24 +128,135 @@ struct Smem {
     }
 };
 
-// Stage NF fields of a ROWS x COLS window starting at (gx0, gz0) into dst.
-template <int NF, int ROWS, int COLS>
-__device__ __forceinline__ void stage(float *dst, const float *const *src, long long off, int gx0, int gz0,
-                                      int nx, int pitch, int tid) {
-    constexpr int C4 = COLS / 4;
-    constexpr int PER = ROWS * C4;
+// Stage NF fields (shared-memory field stride FSTR floats) of a ROWS x COLS
+// window starting at (gx0, gz0) with 16-byte cp.async copies; the chunk
+// geometry is computed once for all fields.  Chunks outside the grid are
+// zero-filled.
+template <int NF, int ROWS, int COLS, int FSTR>
+__device__ __forceinline__ void stage_strided(float *dst, const float *const *src, long long off, int gx0, int gz0,
+                                              int nx, int pitch, int tid) {
+    constexpr int C4 = COLS / 4, PER = ROWS * C4;
+    for (int q = tid; q < PER; q += kThreads) {
+        const int r = q / C4, c = q - r * C4;
+        const int gx = gx0 + r, gz = gz0 + 4 * c;
+        const bool ok = gx >= 0 && gx < nx && gz >= 0 && gz < pitch;
+        const long long o = ok ? off + (long long)gx * pitch + gz : 0;
 #pragma unroll
-    for (int f = 0; f < NF; f++) {
-        const float *base = src[f] + off;
-        for (int q = tid; q < PER; q += kThreads) {
-            int r = q / C4, c = q - r * C4;
-            int gx = gx0 + r, gz = gz0 + 4 * c;
-            bool ok = gx >= 0 && gx < nx && gz >= 0 && gz < pitch;
-            const float *g = ok ? base + (long long)gx * pitch + gz : base;
-            cp_async16(dst + f * ROWS * COLS + r * COLS + 4 * c, g, ok ? 16 : 0);
-        }
+        for (int f = 0; f < NF; f++) cp_async16(dst + f * FSTR + r * COLS + 4 * c, src[f] + o, ok ? 16 : 0);
     }
 }
+
+// Entries of this shot at cells of the computed region, summed per cell in
+// entry order into J (NINJ components, VX x RVZ cells): the source scatter
+// stf_dsy / stf_dsxz (solver.py:78-93).  Returns whether any entry falls in
+// the tile (J is written only then).  Block-wide: every thread must call it.
+template <int NINJ, int VX, int RVZ>
+__device__ __forceinline__ bool scatter_entries(const int *inj_ptr, const int *inj_cell, const int *inj_row,
+                                                const float *const *val_src, int nt, int it, const FastDiv &divnz,
+                                                int nz, int x0, int z0, int shot, float *J, int *sLoc, float *sVal,
+                                                int *sWarp) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    bool has = false;
+    if (!inj_ptr) return false;
+    const int p0 = inj_ptr[shot], p1 = inj_ptr[shot + 1];
+    for (int base = p0; base < p1; base += kThreads) {
+        const int e = base + tid;
+        int loc = -1;
+        float val[NINJ];
+        if (e < p1) {
+            const int k = inj_cell[e];
+            const int gx = fdiv(k, divnz), gz = k - gx * nz;
+            const int rx = gx - (x0 - 1), rz = gz - (z0 - 1);
+            if (rx >= 0 && rx < VX && rz >= 0 && rz < RVZ) {
+                loc = rx * RVZ + rz;
+                const long long src = (long long)inj_row[e] * nt + it;
+#pragma unroll
+                for (int c = 0; c < NINJ; c++) val[c] = val_src[c][src];
+            }
+        }
+        const int n_in = __syncthreads_count(loc >= 0);
+        if (n_in == 0) continue;
+        if (!has) {
+            for (int q = tid; q < NINJ * VX * RVZ; q += kThreads) J[q] = 0.f;
+            has = true;
+        }
+        const unsigned ball = __ballot_sync(0xffffffffu, loc >= 0);
+        if (lane == 0) sWarp[warp] = __popc(ball);
+        __syncthreads();
+        if (loc >= 0) {
+            int pos = __popc(ball & ((1u << lane) - 1u));
+            for (int w = 0; w < warp; w++) pos += sWarp[w];
+            sLoc[pos] = loc;
+#pragma unroll
+            for (int c = 0; c < NINJ; c++) sVal[c * kThreads + pos] = val[c];
+        }
+        __syncthreads();
+        if (tid == 0) {
+            for (int q = 0; q < n_in; q++) {
+#pragma unroll
+                for (int c = 0; c < NINJ; c++) J[c * VX * RVZ + sLoc[q]] += sVal[c * kThreads + q];
+            }
+        }
+        __syncthreads();
+    }
+    return has;
+}
+
+// ---------------------------------------------------------- TMA staging
+// Tensor maps of one step: stress / velocity of the current half and the
+// displacement as 3-D maps (z = pitch, x, shot), the model as 2-D maps.
+struct TmaMaps {
+    CUtensorMap sig[6];
+    CUtensorMap vel[3];
+    CUtensorMap disp[3];
+    CUtensorMap vp[3];  // model fields read on the velocity region
+    CUtensorMap ip[4];  // model fields read on the interior
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, int count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: gives up after ~2^22 polls (each poll may suspend the warp
+// for a while), so a lost transaction ends the kernel instead of hanging it.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    for (int i = 0; i < (1 << 22); i++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int c0, int c1, int c2,
+                                            uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::
+            "r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int c0, int c1, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Device-side status of the TMA kernels (a wait that gave up), read and
+// cleared by fwi_device_status.
+__device__ int g_device_status = 0;
 
 // Staging copies plus the source scatter (stf_dsy / stf_dsxz, solver.py:78-93):
 // entries of this shot inside the computed velocity region are summed per
@@ -156,60 +271,60 @@ __device__ __forceinline__ bool prologue(const StepArgs &a, const Smem<MODE, TX,
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nx = a.nx, nz = a.nz, pitch = a.pitch;
     const long long soff = (long long)shot * nx * pitch;
-    stage<F::NS, SX, SZ>(sm.S, a.sig_in, soff, x0 - 3, z0 - 4, nx, pitch, tid);
-    stage<F::NV, VX, SZ>(sm.V, a.vel_in, soff, x0 - 1, z0 - 4, nx, pitch, tid);
-    stage<F::NVP, VX, SZ>(sm.P, a.vp, 0, x0 - 1, z0 - 4, nx, pitch, tid);
-    stage<F::NV, TX, TZ>(sm.U, a.disp, soff, x0, z0, nx, pitch, tid);
-    stage<F::NIP, TX, TZ>(sm.I, a.ip, 0, x0, z0, nx, pitch, tid);
+    stage_strided<F::NS, SX, SZ, T::FS>(sm.S, a.sig_in, soff, x0 - 3, z0 - 4, nx, pitch, tid);
+    stage_strided<F::NV, VX, SZ, T::FV>(sm.V, a.vel_in, soff, x0 - 1, z0 - 4, nx, pitch, tid);
+    stage_strided<F::NVP, VX, SZ, T::FV>(sm.P, a.vp, 0, x0 - 1, z0 - 4, nx, pitch, tid);
+    stage_strided<F::NV, TX, TZ, TX * TZ>(sm.U, a.disp, soff, x0, z0, nx, pitch, tid);
+    stage_strided<F::NIP, TX, TZ, TX * TZ>(sm.I, a.ip, 0, x0, z0, nx, pitch, tid);
     cp_async_commit();
-
-    bool has_inj = false;
-    if (a.inj_ptr) {
-        const int p0 = a.inj_ptr[shot], p1 = a.inj_ptr[shot + 1];
-        for (int base = p0; base < p1; base += kThreads) {
-            const int e = base + tid;
-            int loc = -1;
-            float val[F::NINJ];
-            if (e < p1) {
-                const int k = a.inj_cell[e];
-                const int gx = fdiv(k, a.divnz), gz = k - gx * nz;
-                const int rx = gx - (x0 - 1), rz = gz - (z0 - 1);
-                if (rx >= 0 && rx < VX && rz >= 0 && rz < RVZ) {
-                    loc = rx * RVZ + rz;
-                    const long long src = (long long)a.inj_row[e] * a.nt + a.it;
-#pragma unroll
-                    for (int c = 0; c < F::NINJ; c++) val[c] = a.stf[c][src];
-                }
-            }
-            const int n_in = __syncthreads_count(loc >= 0);
-            if (n_in == 0) continue;
-            if (!has_inj) {
-                for (int q = tid; q < T::J_SZ; q += kThreads) sm.J[q] = 0.f;
-                has_inj = true;
-            }
-            const unsigned ball = __ballot_sync(0xffffffffu, loc >= 0);
-            if (lane == 0) sm.warp[warp] = __popc(ball);
-            __syncthreads();
-            if (loc >= 0) {
-                int pos = __popc(ball & ((1u << lane) - 1u));
-                for (int w = 0; w < warp; w++) pos += sm.warp[w];
-                sm.loc[pos] = loc;
-#pragma unroll
-                for (int c = 0; c < F::NINJ; c++) sm.val[c * kThreads + pos] = val[c];
-            }
-            __syncthreads();
-            if (tid == 0) {
-                for (int q = 0; q < n_in; q++) {
-#pragma unroll
-                    for (int c = 0; c < F::NINJ; c++) sm.J[c * VX * RVZ + sm.loc[q]] += sm.val[c * kThreads + q];
-                }
-            }
-            __syncthreads();
-        }
-    }
+    const bool has_inj = scatter_entries<F::NINJ, VX, RVZ>(a.inj_ptr, a.inj_cell, a.inj_row, a.stf, a.nt, a.it,
+                                                           a.divnz, nz, x0, z0, shot, sm.J, sm.loc, sm.val, sm.warp);
+    (void)lane;
+    (void)warp;
     cp_async_wait_all();
     __syncthreads();
     return has_inj;
+}
+
+// The same staging with TMA: one thread issues one tensor copy per field
+// (zero fill outside the grid comes from the tensor maps), completion is
+// counted on an mbarrier, and the source scatter overlaps the copies.  Returns
+// -1 if the wait gave up (the kernel must then return), else has_inj.
+template <int MODE, int TX, int TZ>
+__device__ __forceinline__ int prologue_tma(const StepArgs &a, const TmaMaps &m, const Smem<MODE, TX, TZ> &sm,
+                                            uint64_t *bar, int x0, int z0, int shot) {
+    using T = Tile<MODE, TX, TZ>;
+    using F = Fields<MODE>;
+    constexpr int SX = T::SX, SZ = T::SZ, VX = T::VX, RVZ = T::RVZ;
+    constexpr uint32_t bytes = 4u * (F::NS * SX * SZ + (F::NV + F::NVP) * VX * SZ + (F::NV + F::NIP) * TX * TZ);
+    static_assert(bytes < (1u << 20), "mbarrier transaction count limit");
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_expect_tx(bar, bytes);
+#pragma unroll
+        for (int f = 0; f < F::NS; f++) tma_load_3d(sm.S + f * T::FS, &m.sig[f], z0 - 4, x0 - 3, shot, bar);
+#pragma unroll
+        for (int q = 0; q < F::NV; q++) tma_load_3d(sm.V + q * T::FV, &m.vel[q], z0 - 4, x0 - 1, shot, bar);
+#pragma unroll
+        for (int p = 0; p < F::NVP; p++) tma_load_2d(sm.P + p * T::FV, &m.vp[p], z0 - 4, x0 - 1, bar);
+#pragma unroll
+        for (int q = 0; q < F::NV; q++) tma_load_3d(sm.U + q * TX * TZ, &m.disp[q], z0, x0, shot, bar);
+#pragma unroll
+        for (int p = 0; p < F::NIP; p++) tma_load_2d(sm.I + p * TX * TZ, &m.ip[p], z0, x0, bar);
+    }
+    const bool has_inj = scatter_entries<F::NINJ, VX, RVZ>(a.inj_ptr, a.inj_cell, a.inj_row, a.stf, a.nt, a.it,
+                                                           a.divnz, a.nz, x0, z0, shot, sm.J, sm.loc, sm.val, sm.warp);
+    const bool ok = mbar_wait(bar, 0);
+    if (__syncthreads_or(!ok)) {  // block-uniform decision
+        if (threadIdx.x == 0) atomicExch(&g_device_status, 1);
+        if (!ok) mbar_wait(bar, 0);  // one more bounded chance for the copies in flight to land
+        return -1;
+    }
+    return has_inj ? 1 : 0;
 }
 
 // Velocity update of one cell from its stress divergence ds (all in shared
@@ -226,12 +341,12 @@ __device__ __forceinline__ void velocity_update(const Smem<MODE, TX, TZ> &sm, in
         for (int c = 0; c < F::NINJ; c++) ds[c] += sm.J[c * VX * RVZ + rx * RVZ + rz];
     }
     const int vi = rx * SZ + rz + 3;
-    const float buo = sm.P[vi], bnd = sm.P[VX * SZ + vi];
+    const float buo = sm.P[vi], bnd = sm.P[T::FV + vi];
 #pragma unroll
     for (int c = 0; c < F::NV; c++) {
-        const float b = (MODE == FWI_SPIN && c == 2) ? sm.P[2 * VX * SZ + vi] : buo;
-        const float v = bnd * (sm.V[c * VX * SZ + vi] + ds[c] * b);
-        sm.V[c * VX * SZ + vi] = v;
+        const float b = (MODE == FWI_SPIN && c == 2) ? sm.P[2 * T::FV + vi] : buo;
+        const float v = bnd * (sm.V[c * T::FV + vi] + ds[c] * b);
+        sm.V[c * T::FV + vi] = v;
         vnew[c] = v;
     }
 }
@@ -260,7 +375,7 @@ template <int MODE, int TX, int TZ, class DXP, class DZP>
 __device__ __forceinline__ void stress_update(const StepArgs &a, const float *s0, const float *ip, float vyc, long long g,
                                               DXP dxp, DZP dzp) {
     using T = Tile<MODE, TX, TZ>;
-    constexpr int FS = T::SX * T::SZ, FI = TX * TZ;
+    constexpr int FS = T::FS, FI = TX * TZ;
     const float dt = a.dt;
     if (MODE == FWI_SH) {
         const float dm = dt * ip[0];
@@ -329,7 +444,7 @@ __device__ __forceinline__ bool velocity_cell(const StepArgs &a, const Smem<MODE
     const int cz = rz + 3;
     if (gx < 0 || gx >= a.nx || gz < 0 || gz >= a.nz) {
 #pragma unroll
-        for (int c = 0; c < Fields<MODE>::NV; c++) sm.V[c * VX * SZ + rx * SZ + cz] = 0.f;
+        for (int c = 0; c < Fields<MODE>::NV; c++) sm.V[c * T::FV + rx * SZ + cz] = 0.f;
         return false;
     }
     const bool okx = gx >= 2 && gx < a.nx - 2, okz = gz >= 2 && gz < a.nz - 2;
@@ -337,15 +452,15 @@ __device__ __forceinline__ bool velocity_cell(const StepArgs &a, const Smem<MODE
     const float cx1 = a.cx1, cx2 = a.cx2, cz1 = a.cz1, cz2 = a.cz2;
     auto dxm = [&](int f) -> float {
         if (!okx) return 0.f;
-        const float *s = s0 + f * SX * SZ;
+        const float *s = s0 + f * T::FS;
         return cx1 * (s[0] - s[-SZ]) - cx2 * (s[SZ] - s[-2 * SZ]);
     };
     auto dzm = [&](int f) -> float {
         if (!okz) return 0.f;
-        const float *s = s0 + f * SX * SZ;
+        const float *s = s0 + f * T::FS;
         return cz1 * (s[0] - s[-1]) - cz2 * (s[1] - s[-2]);
     };
-    auto center = [&](int f) -> float { return s0[f * SX * SZ]; };
+    auto center = [&](int f) -> float { return s0[f * T::FS]; };
     divergence<MODE>(dxm, dzm, center, ds);
     velocity_update<MODE, TX, TZ>(sm, rx, rz, ds, has_inj, v);
     return true;
@@ -380,7 +495,7 @@ template <int MODE, int TX, int TZ>
 __global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 2) step_kernel(const StepArgs a) {
     using T = Tile<MODE, TX, TZ>;
     constexpr int SX = T::SX, SZ = T::SZ, VX = T::VX;
-    extern __shared__ __align__(16) float smem[];
+    extern __shared__ __align__(128) float smem[];
     const Smem<MODE, TX, TZ> sm(smem);
     const int z0 = blockIdx.x * TZ, x0 = blockIdx.y * TX, shot = blockIdx.z;
     const int nx = a.nx, nz = a.nz, pitch = a.pitch;
@@ -406,15 +521,15 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 2) step_kerne
         const float *v0 = sm.V + (ix + 1) * SZ + (iz + 4);
         auto dxp = [&](int f) -> float {
             if (!okx) return 0.f;
-            const float *v = v0 + f * VX * SZ;
+            const float *v = v0 + f * T::FV;
             return cx1 * (v[SZ] - v[0]) - cx2 * (v[2 * SZ] - v[-SZ]);
         };
         auto dzp = [&](int f) -> float {
             if (!okz) return 0.f;
-            const float *v = v0 + f * VX * SZ;
+            const float *v = v0 + f * T::FV;
             return cz1 * (v[1] - v[0]) - cz2 * (v[2] - v[-1]);
         };
-        const float vyc = MODE == FWI_SPIN ? v0[2 * VX * SZ] : 0.f;
+        const float vyc = MODE == FWI_SPIN ? v0[2 * T::FV] : 0.f;
         stress_update<MODE, TX, TZ>(a, sm.S + (ix + 3) * SZ + (iz + 4), sm.I + c, vyc,
                                     soff + (long long)gx * pitch + gz, dxp, dzp);
     }
@@ -423,19 +538,28 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 2) step_kerne
 
 // -------------------------------------------------- register-window mapping
 
-template <int MODE, int TX>
-__global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 3) step_kernel_rw(const StepArgs a) {
+template <int MODE, int TX, bool TMA>
+__global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 3)
+    step_kernel_rw(const __grid_constant__ StepArgs a, const __grid_constant__ TmaMaps maps) {
     constexpr int TZ = 32, RPW = TX / (kThreads / 32);
     static_assert(RPW >= 1 && RPW * (kThreads / 32) == TX, "TX must be a multiple of the warp count");
     using T = Tile<MODE, TX, TZ>;
     using F = Fields<MODE>;
     constexpr int SX = T::SX, SZ = T::SZ, VX = T::VX;
-    extern __shared__ __align__(16) float smem[];
+    extern __shared__ __align__(128) float smem[];
     const Smem<MODE, TX, TZ> sm(smem);
     const int z0 = blockIdx.x * TZ, x0 = blockIdx.y * TX, shot = blockIdx.z;
     const int nx = a.nx, nz = a.nz, pitch = a.pitch;
     const long long soff = (long long)shot * nx * pitch;
-    const bool has_inj = prologue<MODE, TX, TZ>(a, sm, x0, z0, shot);
+    bool has_inj;
+    if constexpr (TMA) {
+        const int r = prologue_tma<MODE, TX, TZ>(a, maps, sm, reinterpret_cast<uint64_t *>(smem + T::BAR_OFF), x0,
+                                                 z0, shot);
+        if (r < 0) return;
+        has_inj = r > 0;
+    } else {
+        has_inj = prologue<MODE, TX, TZ>(a, sm, x0, z0, shot);
+    }
 
     const int lane = threadIdx.x & 31, ix0 = (threadIdx.x >> 5) * RPW;
     const int gz = z0 + lane, col = lane + 4;
@@ -451,7 +575,7 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 3) step_kerne
         for (int f = 0; f < F::NS; f++)
             if (takes_dxm(MODE, f)) {
 #pragma unroll
-                for (int r = 0; r < RPW + 3; r++) w[f][r] = sm.S[f * SX * SZ + (ix0 + 1 + r) * SZ + col];
+                for (int r = 0; r < RPW + 3; r++) w[f][r] = sm.S[f * T::FS + (ix0 + 1 + r) * SZ + col];
             }
 #pragma unroll
         for (int q = 0; q < RPW; q++) {
@@ -459,7 +583,7 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 3) step_kerne
             const int vi = (ix + 1) * SZ + col;
             if (!(zin && gx < nx)) {
 #pragma unroll
-                for (int c = 0; c < F::NV; c++) sm.V[c * VX * SZ + vi] = 0.f;
+                for (int c = 0; c < F::NV; c++) sm.V[c * T::FV + vi] = 0.f;
                 continue;
             }
             const bool okx = gx >= 2 && gx < nx - 2;
@@ -467,10 +591,10 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 3) step_kerne
             auto dxm = [&](int f) -> float {
                 return okx ? cx1 * (w[f][q + 2] - w[f][q + 1]) - cx2 * (w[f][q + 3] - w[f][q]) : 0.f;
             };
-            auto center = [&](int f) -> float { return takes_dxm(MODE, f) ? w[f][q + 2] : srow[f * SX * SZ]; };
+            auto center = [&](int f) -> float { return takes_dxm(MODE, f) ? w[f][q + 2] : srow[f * T::FS]; };
             auto dzm = [&](int f) -> float {
                 if (!okz) return 0.f;
-                const float *s = srow + f * SX * SZ;
+                const float *s = srow + f * T::FS;
                 return cz1 * (center(f) - s[-1]) - cz2 * (s[1] - s[-2]);
             };
             float ds[3], v[3];
@@ -491,7 +615,7 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 3) step_kerne
 #pragma unroll
         for (int f = 0; f < F::NV; f++) {
 #pragma unroll
-            for (int r = 0; r < RPW + 3; r++) w[f][r] = sm.V[f * VX * SZ + (ix0 + r) * SZ + col];
+            for (int r = 0; r < RPW + 3; r++) w[f][r] = sm.V[f * T::FV + (ix0 + r) * SZ + col];
         }
 #pragma unroll
         for (int q = 0; q < RPW; q++) {
@@ -504,7 +628,7 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 3) step_kerne
             };
             auto dzp = [&](int f) -> float {
                 if (!okz) return 0.f;
-                const float *v = vrow + f * VX * SZ;
+                const float *v = vrow + f * T::FV;
                 return cz1 * (v[1] - w[f][q + 1]) - cz2 * (v[2] - v[-1]);
             };
             const float vyc = MODE == FWI_SPIN ? w[F::NV - 1][q + 1] : 0.f;
@@ -563,83 +687,13 @@ struct AdjTile {
     static constexpr size_t bytes = sizeof(float) * (size_t)(S_SZ + V_SZ + J_SZ + LIST);
 };
 
-// Stage NF fields (field stride FSTR floats) of a ROWS x COLS window.
-template <int NF, int ROWS, int COLS, int FSTR>
-__device__ __forceinline__ void stage_strided(float *dst, const float *const *src, long long off, int gx0, int gz0,
-                                              int nx, int pitch, int tid) {
-    constexpr int C4 = COLS / 4, PER = ROWS * C4;
-    for (int q = tid; q < PER; q += kThreads) {
-        const int r = q / C4, c = q - r * C4;
-        const int gx = gx0 + r, gz = gz0 + 4 * c;
-        const bool ok = gx >= 0 && gx < nx && gz >= 0 && gz < pitch;
-        const long long o = ok ? off + (long long)gx * pitch + gz : 0;
-#pragma unroll
-        for (int f = 0; f < NF; f++) cp_async16(dst + f * FSTR + r * COLS + 4 * c, src[f] + o, ok ? 16 : 0);
-    }
-}
-
-// Entries of this shot at cells of the computed region, summed per cell in
-// entry order into J (NINJ components, VX x RVZ cells).  Returns whether any
-// entry falls in the tile.
-template <int NINJ, int VX, int RVZ>
-__device__ __forceinline__ bool scatter_entries(const int *inj_ptr, const int *inj_cell, const int *inj_row,
-                                                const float *const *val_src, int nt, int it, const FastDiv &divnz,
-                                                int nz, int x0, int z0, int shot, float *J, int *sLoc, float *sVal,
-                                                int *sWarp) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    bool has = false;
-    if (!inj_ptr) return false;
-    const int p0 = inj_ptr[shot], p1 = inj_ptr[shot + 1];
-    for (int base = p0; base < p1; base += kThreads) {
-        const int e = base + tid;
-        int loc = -1;
-        float val[NINJ];
-        if (e < p1) {
-            const int k = inj_cell[e];
-            const int gx = fdiv(k, divnz), gz = k - gx * nz;
-            const int rx = gx - (x0 - 1), rz = gz - (z0 - 1);
-            if (rx >= 0 && rx < VX && rz >= 0 && rz < RVZ) {
-                loc = rx * RVZ + rz;
-                const long long src = (long long)inj_row[e] * nt + it;
-#pragma unroll
-                for (int c = 0; c < NINJ; c++) val[c] = val_src[c][src];
-            }
-        }
-        const int n_in = __syncthreads_count(loc >= 0);
-        if (n_in == 0) continue;
-        if (!has) {
-            for (int q = tid; q < NINJ * VX * RVZ; q += kThreads) J[q] = 0.f;
-            has = true;
-        }
-        const unsigned ball = __ballot_sync(0xffffffffu, loc >= 0);
-        if (lane == 0) sWarp[warp] = __popc(ball);
-        __syncthreads();
-        if (loc >= 0) {
-            int pos = __popc(ball & ((1u << lane) - 1u));
-            for (int w = 0; w < warp; w++) pos += sWarp[w];
-            sLoc[pos] = loc;
-#pragma unroll
-            for (int c = 0; c < NINJ; c++) sVal[c * kThreads + pos] = val[c];
-        }
-        __syncthreads();
-        if (tid == 0) {
-            for (int q = 0; q < n_in; q++) {
-#pragma unroll
-                for (int c = 0; c < NINJ; c++) J[c * VX * RVZ + sLoc[q]] += sVal[c * kThreads + q];
-            }
-        }
-        __syncthreads();
-    }
-    return has;
-}
-
 template <int MODE, int TX, int TZ>
 __global__ void __launch_bounds__(kThreads, 2) adjoint_kernel(const AdjArgs a) {
     using T = AdjTile<MODE, TX, TZ>;
     using F = Fields<MODE>;
     constexpr int SX = T::SX, SZ = T::SZ, VX = T::VX, RVZ = T::RVZ, FS = T::FS, FV = T::FV;
     constexpr int NS = F::NS, NV = F::NV, NL = T::NL;
-    extern __shared__ __align__(16) float smem[];
+    extern __shared__ __align__(128) float smem[];
     float *sSig = smem, *sL = sSig + NS * FS, *sT = sL + NL * FS;
     float *sV = sT + T::NTT * FS, *sU = sV + NV * FV, *sB = sU + NV * FV;
     float *sJ = sB + 2 * FV;
@@ -894,43 +948,112 @@ struct TileShape {
     int tx, tz, rw;
 };
 // Variants selectable through fwi_batch.tile; 0 is the default.
-static const TileShape kTiles[] = {{32, 32, 1}, {32, 32, 0}, {16, 64, 0}, {16, 32, 0}, {64, 32, 0},
-                                   {8, 64, 0},  {32, 32, 1}, {16, 32, 1}, {64, 32, 1}};
+// rw: 0 generic mapping, 1 register window + cp.async, 2 register window + TMA
+static const TileShape kTiles[] = {{16, 32, 1}, {32, 32, 0}, {16, 64, 0}, {16, 32, 0}, {64, 32, 0}, {8, 64, 0},
+                                   {32, 32, 1}, {16, 32, 1}, {64, 32, 1}, {32, 32, 2}, {16, 32, 2}, {8, 32, 2}};
 constexpr int kNumTiles = sizeof(kTiles) / sizeof(kTiles[0]);
 
-template <int MODE, int TX, int TZ, bool RW>
+// cuTensorMapEncodeTiled, fetched from the driver at run time.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// Tiled float32 map over a [nshots][nx][pitch] block (rank 3) or an
+// [nx][pitch] model array (rank 2), box (bz, bx), zero fill outside.
+static int encode_map(CUtensorMap *m, const float *base, int rank, int pitch, int nx, int nshots, int bz, int bx) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return set_error(FWI_ECUDA, "cuTensorMapEncodeTiled unavailable from the driver");
+    cuuint64_t dims[3] = {(cuuint64_t)pitch, (cuuint64_t)nx, (cuuint64_t)(nshots < 1 ? 1 : nshots)};
+    cuuint64_t strides[2] = {(cuuint64_t)pitch * 4, (cuuint64_t)pitch * (cuuint64_t)nx * 4};
+    cuuint32_t box[3] = {(cuuint32_t)bz, (cuuint32_t)bx, 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (cuuint32_t)rank, const_cast<float *>(base), dims, strides,
+                    box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(FWI_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return 0;
+}
+
+template <int MODE, int TX, int TZ>
+static int build_maps(const StepArgs &a, int nshots, TmaMaps &m) {
+    using T = Tile<MODE, TX, TZ>;
+    using F = Fields<MODE>;
+    int rc = 0;
+    for (int f = 0; f < F::NS && !rc; f++) rc = encode_map(&m.sig[f], a.sig_in[f], 3, a.pitch, a.nx, nshots, T::SZ, T::SX);
+    for (int q = 0; q < F::NV && !rc; q++) rc = encode_map(&m.vel[q], a.vel_in[q], 3, a.pitch, a.nx, nshots, T::SZ, T::VX);
+    for (int q = 0; q < F::NV && !rc; q++) rc = encode_map(&m.disp[q], a.disp[q], 3, a.pitch, a.nx, nshots, TZ, TX);
+    for (int p = 0; p < F::NVP && !rc; p++) rc = encode_map(&m.vp[p], a.vp[p], 2, a.pitch, a.nx, 1, T::SZ, T::VX);
+    for (int p = 0; p < F::NIP && !rc; p++) rc = encode_map(&m.ip[p], a.ip[p], 2, a.pitch, a.nx, 1, TZ, TX);
+    return rc;
+}
+
+// kind: 0 generic mapping, 1 register window (cp.async), 2 register window (TMA)
+template <int MODE, int TX, int TZ, int KIND>
 static int launch_tile(const StepArgs &a, int nshots, cudaStream_t st) {
     using T = Tile<MODE, TX, TZ>;
-    void (*kern)(const StepArgs);
-    if constexpr (RW) {
-        static_assert(TZ == 32, "the register-window mapping has one lane per z column");
-        kern = step_kernel_rw<MODE, TX>;
-    } else {
-        kern = step_kernel<MODE, TX, TZ>;
-    }
     static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::bytes);
-        if (e != cudaSuccess) return set_error(FWI_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
-        attr_set = true;
+    static TmaMaps none;  // unused by the cp.async variants
+    if constexpr (KIND == 0) {
+        if (!attr_set) {
+            cudaError_t e = cudaFuncSetAttribute(step_kernel<MODE, TX, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)T::bytes);
+            if (e != cudaSuccess) return set_error(FWI_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+            attr_set = true;
+        }
+        dim3 grid((a.nz + TZ - 1) / TZ, (a.nx + TX - 1) / TX, nshots);
+        step_kernel<MODE, TX, TZ><<<grid, kThreads, T::bytes, st>>>(a);
+    } else {
+        static_assert(TZ == 32, "the register-window mapping has one lane per z column");
+        constexpr bool TMA = KIND == 2;
+        if (!attr_set) {
+            cudaError_t e = cudaFuncSetAttribute(step_kernel_rw<MODE, TX, TMA>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::bytes);
+            if (e != cudaSuccess) return set_error(FWI_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+            attr_set = true;
+        }
+        const TmaMaps *maps = &none;
+        TmaMaps built;
+        if constexpr (TMA) {
+            int rc = build_maps<MODE, TX, TZ>(a, nshots, built);
+            if (rc) return rc;
+            maps = &built;
+        }
+        dim3 grid((a.nz + TZ - 1) / TZ, (a.nx + TX - 1) / TX, nshots);
+        step_kernel_rw<MODE, TX, TMA><<<grid, kThreads, T::bytes, st>>>(a, *maps);
     }
-    dim3 grid((a.nz + TZ - 1) / TZ, (a.nx + TX - 1) / TX, nshots);
-    kern<<<grid, kThreads, T::bytes, st>>>(a);
     return check_launch("step_kernel");
 }
 
 template <int MODE>
 static int launch_mode(const StepArgs &a, int nshots, int tile, cudaStream_t st) {
     switch (tile) {
-        case 0: return launch_tile<MODE, 32, 32, true>(a, nshots, st);
-        case 1: return launch_tile<MODE, 32, 32, false>(a, nshots, st);
-        case 2: return launch_tile<MODE, 16, 64, false>(a, nshots, st);
-        case 3: return launch_tile<MODE, 16, 32, false>(a, nshots, st);
-        case 4: return launch_tile<MODE, 64, 32, false>(a, nshots, st);
-        case 5: return launch_tile<MODE, 8, 64, false>(a, nshots, st);
-        case 6: return launch_tile<MODE, 32, 32, true>(a, nshots, st);
-        case 7: return launch_tile<MODE, 16, 32, true>(a, nshots, st);
-        case 8: return launch_tile<MODE, 64, 32, true>(a, nshots, st);
+        case 0: return launch_tile<MODE, 16, 32, 1>(a, nshots, st);
+        case 1: return launch_tile<MODE, 32, 32, 0>(a, nshots, st);
+        case 2: return launch_tile<MODE, 16, 64, 0>(a, nshots, st);
+        case 3: return launch_tile<MODE, 16, 32, 0>(a, nshots, st);
+        case 4: return launch_tile<MODE, 64, 32, 0>(a, nshots, st);
+        case 5: return launch_tile<MODE, 8, 64, 0>(a, nshots, st);
+        case 6: return launch_tile<MODE, 32, 32, 1>(a, nshots, st);
+        case 7: return launch_tile<MODE, 16, 32, 1>(a, nshots, st);
+        case 8: return launch_tile<MODE, 64, 32, 1>(a, nshots, st);
+        case 9: return launch_tile<MODE, 32, 32, 2>(a, nshots, st);
+        case 10: return launch_tile<MODE, 16, 32, 2>(a, nshots, st);
+        case 11: return launch_tile<MODE, 8, 32, 2>(a, nshots, st);
     }
     return set_error(FWI_EINVAL, "unknown tile variant %d", tile);
 }
