@@ -295,8 +295,7 @@ def main():
     def tune():
         from seispie_b200.autotune import autotune
         best, times = autotune(m_init, nshots, nt, rid, inj, stf)
-        return best, times[best], {"%dx%d%s" % (*_lib.tile_shape(t), "" if t in (1, 2, 3, 4, 5) else "rw"): ms
-                                   for t, ms in times.items()}
+        return best, times[best], {_lib.tile_label(t): ms for t, ms in times.items()}
 
     tuned = None
     if a.autotune:
@@ -364,7 +363,7 @@ def main():
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
 
     if rank == 0:
-        extra = {"tile": _lib.tile_shape(b_tile(a, tuned)), "misfit": misfit_total}
+        extra = {"tile": _lib.tile_label(b_tile(a, tuned)), "misfit": misfit_total}
         if tuned:
             extra["autotune_ms_per_fwd_step"] = tuned[2]
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,

@@ -126,6 +126,13 @@ int fwi_last_error(char *buf, size_t len);
  * a 1-D grid of threads_per_block threads, fd2d.py:184-187). */
 int fwi_tile_shape(int tile, int *tx, int *tz);
 
+/* Kind of step-kernel variant `tile`: 0 = one thread per cell walking the
+ * tile, staged with cp.async; 1 = lane per z column with an x register
+ * window, staged with cp.async; 2 = the same staged with TMA tensor copies
+ * (cp.async.bulk.tensor, mbarrier completion).  FWI_EINVAL if unknown.  No
+ * counterpart in the reference. */
+int fwi_tile_kind(int tile);
+
 /* vp/vs -> lambda/mu in place: lam_io holds vp and mu_io holds vs on entry.
  * Replaces vps2lm, seispie/solver/fd2d/fd2d.py:21-33 (launched at
  * fd2d.py:216).  n elements, any layout. */

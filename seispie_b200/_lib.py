@@ -64,6 +64,7 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
         "fwi_launch_count": ([], ctypes.c_longlong),
         "fwi_last_error": ([ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
         "fwi_tile_shape": ([ctypes.c_int, _ip, _ip], ctypes.c_int),
+        "fwi_tile_kind": ([ctypes.c_int], ctypes.c_int),
         "fwi_vps2lm": ([_vp, _vp, _vp, ctypes.c_longlong, _vp], ctypes.c_int),
         "fwi_lm2vps": ([_vp, _vp, _vp, ctypes.c_longlong, _vp], ctypes.c_int),
         "fwi_set_bound": ([_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
@@ -118,6 +119,13 @@ def tile_shape(tile: int) -> tuple[int, int]:
     x, z = ctypes.c_int(), ctypes.c_int()
     check(load().fwi_tile_shape(tile, ctypes.byref(x), ctypes.byref(z)), "fwi_tile_shape")
     return x.value, z.value
+
+
+def tile_label(tile: int) -> str:
+    """e.g. '9:32x32/tma' -- variant id, interior tile and staging kind."""
+    tx, tz = tile_shape(tile)
+    kind = {0: "generic", 1: "rw", 2: "tma"}[load().fwi_tile_kind(tile)]
+    return "%d:%dx%d/%s" % (tile, tx, tz, kind)
 
 
 def check(rc: int, what: str = "") -> None:

@@ -50,6 +50,7 @@ int launch_prepare(const float *rho, const float *jr, const float *muc, const fl
                    float *buo, float *buo_j, float *mnc, cudaStream_t st);
 int tile_count();
 bool tile_shape(int tile, int *tx, int *tz);
+int tile_kind(int tile);
 
 static bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
 
@@ -127,6 +128,11 @@ int fwi_last_error(char *buf, size_t len) {
         buf[len - 1] = '\0';
     }
     return g_code;
+}
+
+int fwi_tile_kind(int tile) {
+    const int k = tile_kind(tile);
+    return k < 0 ? set_error(FWI_EINVAL, "tile variant %d unknown", tile) : k;
 }
 
 int fwi_tile_shape(int tile, int *tx, int *tz) {

@@ -949,7 +949,7 @@ struct TileShape {
 };
 // Variants selectable through fwi_batch.tile; 0 is the default.
 // rw: 0 generic mapping, 1 register window + cp.async, 2 register window + TMA
-static const TileShape kTiles[] = {{16, 32, 1}, {32, 32, 0}, {16, 64, 0}, {16, 32, 0}, {64, 32, 0}, {8, 64, 0},
+static const TileShape kTiles[] = {{32, 32, 2}, {32, 32, 0}, {16, 64, 0}, {16, 32, 0}, {64, 32, 0}, {8, 64, 0},
                                    {32, 32, 1}, {16, 32, 1}, {64, 32, 1}, {32, 32, 2}, {16, 32, 2}, {8, 32, 2}};
 constexpr int kNumTiles = sizeof(kTiles) / sizeof(kTiles[0]);
 
@@ -1042,7 +1042,7 @@ static int launch_tile(const StepArgs &a, int nshots, cudaStream_t st) {
 template <int MODE>
 static int launch_mode(const StepArgs &a, int nshots, int tile, cudaStream_t st) {
     switch (tile) {
-        case 0: return launch_tile<MODE, 16, 32, 1>(a, nshots, st);
+        case 0: return launch_tile<MODE, 32, 32, 2>(a, nshots, st);
         case 1: return launch_tile<MODE, 32, 32, 0>(a, nshots, st);
         case 2: return launch_tile<MODE, 16, 64, 0>(a, nshots, st);
         case 3: return launch_tile<MODE, 16, 32, 0>(a, nshots, st);
@@ -1066,6 +1066,8 @@ bool tile_shape(int tile, int *tx, int *tz) {
     *tz = kTiles[tile].tz;
     return true;
 }
+
+int tile_kind(int tile) { return (tile < 0 || tile >= kNumTiles) ? -1 : kTiles[tile].rw; }
 
 // Fill the per-step arguments shared by every step of a run.
 static void base_args(const fwi_batch *b, StepArgs &a) {

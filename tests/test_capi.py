@@ -75,7 +75,7 @@ def test_other_entry_points_validate():
     assert lib.fwi_prepare_model(8, None, None, None, 1.0, 4, 8, 8, None, None) == -1
     assert lib.fwi_tile_shape(99, None, None) == -1
     assert lib.fwi_tile_shape(0, None, None) == 0
-    assert _lib.tile_shape(0) == (16, 32)
+    assert _lib.tile_shape(0) == (32, 32) and lib.fwi_tile_kind(0) == 2
     assert len(_lib.tile_variants()) >= 3
 
 
