@@ -173,6 +173,21 @@ int fwi_prepare_model(const float *rho, const float *j, const float *mu_c, const
  * as clear_wavefields does (fd2d.py:318-341).  b->cur is updated. */
 int fwi_run(fwi_batch *b, int adjoint, int it0, int nsteps, void *stream);
 
+/* Uneven batches: n independent forward batches of one mode (each with its
+ * own grid, model, shots, sources, receivers and nt) stepped together, one
+ * launch per time step covering every tile of every running instance.  All
+ * start at the same step with the same `cur`; an instance stops after its
+ * own nt steps.  workspace: caller device buffer of
+ * fwi_multi_workspace_bytes(n) bytes; fwi_multi_prepare uploads the
+ * per-instance step arguments into it (synchronously; call it outside stream
+ * capture, again whenever a pointer changes) and fwi_multi_run enqueues
+ * steps [it0, it0+nsteps) and updates each batch's cur.  Tile variants:
+ * 0 or a 32-column register-window variant.  No counterpart in the reference,
+ * which runs one model at a time (solver.py:352-373). */
+long long fwi_multi_workspace_bytes(int n);
+int fwi_multi_prepare(fwi_batch *const *batches, int n, void *workspace);
+int fwi_multi_run(fwi_batch *const *batches, int n, void *workspace, int it0, int nsteps, void *stream);
+
 /* Exact discrete adjoint of fwi_run's SH / P-SV forward step, run backwards
  * over forward steps it = it_hi-1 down to it_hi-nsteps on the adjoint state
  * held in the batch's wavefield buffers (sig~, v~, u~; cleared by the caller

@@ -74,6 +74,10 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
                               ctypes.c_int),
         "fwi_run": ([ctypes.POINTER(FwiBatch), ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp], ctypes.c_int),
         "fwi_run_transposed": ([ctypes.POINTER(FwiBatch), ctypes.c_int, ctypes.c_int, _vp], ctypes.c_int),
+        "fwi_multi_workspace_bytes": ([ctypes.c_int], ctypes.c_longlong),
+        "fwi_multi_prepare": ([ctypes.POINTER(ctypes.POINTER(FwiBatch)), ctypes.c_int, _vp], ctypes.c_int),
+        "fwi_multi_run": ([ctypes.POINTER(ctypes.POINTER(FwiBatch)), ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int,
+                           _vp], ctypes.c_int),
         "fwi_misfit": ([_vp, _vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _vp],
                        ctypes.c_int),
         "fwi_misfit_partials": ([ctypes.c_int, ctypes.c_int], ctypes.c_longlong),

@@ -36,6 +36,9 @@ int launch_step(const fwi_batch *b, int adjoint, int it, bool snap_u_next, int s
                 int snap_v_slot, cudaStream_t st);
 int launch_interaction(const fwi_batch *b, int isae, cudaStream_t st);
 int launch_adjoint_step(const fwi_batch *b, int it, cudaStream_t st);
+long long multi_workspace_bytes(int n);
+int multi_prepare(fwi_batch *const *bs, int n, void *ws, int (*check)(const fwi_batch *, int, int, int));
+int multi_run(fwi_batch *const *bs, int n, void *ws, int it0, int nsteps, cudaStream_t st);
 int launch_misfit(const float *data, const float *syn, float *adstf, double *misfit, double *partial, int nshots,
                   int nrec, int nt, double dt, cudaStream_t st);
 long long misfit_partials(int nrec, int nt);
@@ -244,6 +247,16 @@ int fwi_run_transposed(fwi_batch *b, int it_hi, int nsteps, void *stream) {
         b->cur ^= 1;
     }
     return 0;
+}
+
+long long fwi_multi_workspace_bytes(int n) { return multi_workspace_bytes(n); }
+
+int fwi_multi_prepare(fwi_batch *const *batches, int n, void *workspace) {
+    return multi_prepare(batches, n, workspace, check_batch);
+}
+
+int fwi_multi_run(fwi_batch *const *batches, int n, void *workspace, int it0, int nsteps, void *stream) {
+    return multi_run(batches, n, workspace, it0, nsteps, (cudaStream_t)stream);
 }
 
 long long fwi_misfit_partials(int nrec, int nt) { return misfit_partials(nrec, nt); }

@@ -539,16 +539,26 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 2) step_kerne
 // -------------------------------------------------- register-window mapping
 
 template <int MODE, int TX, bool TMA>
+__device__ __forceinline__ void rw_body(const StepArgs &a, const TmaMaps &maps, float *smem, int x0, int z0,
+                                        int shot);
+
+template <int MODE, int TX, bool TMA>
 __global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 3)
     step_kernel_rw(const __grid_constant__ StepArgs a, const __grid_constant__ TmaMaps maps) {
+    extern __shared__ __align__(128) float smem[];
+    rw_body<MODE, TX, TMA>(a, maps, smem, blockIdx.y * TX, blockIdx.x * 32, blockIdx.z);
+}
+
+// Body of the register-window step for the tile (x0, z0) of `shot`.
+template <int MODE, int TX, bool TMA>
+__device__ __forceinline__ void rw_body(const StepArgs &a, const TmaMaps &maps, float *smem, int x0, int z0,
+                                        int shot) {
     constexpr int TZ = 32, RPW = TX / (kThreads / 32);
     static_assert(RPW >= 1 && RPW * (kThreads / 32) == TX, "TX must be a multiple of the warp count");
     using T = Tile<MODE, TX, TZ>;
     using F = Fields<MODE>;
     constexpr int SX = T::SX, SZ = T::SZ, VX = T::VX;
-    extern __shared__ __align__(128) float smem[];
     const Smem<MODE, TX, TZ> sm(smem);
-    const int z0 = blockIdx.x * TZ, x0 = blockIdx.y * TX, shot = blockIdx.z;
     const int nx = a.nx, nz = a.nz, pitch = a.pitch;
     const long long soff = (long long)shot * nx * pitch;
     bool has_inj;
@@ -636,6 +646,55 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 3)
                                         soff + (long long)gx * pitch + gz, dxp, dzp);
         }
     }
+}
+
+// ------------------------------------------- uneven multi-instance batches
+//
+// Independent instances (each its own grid, model, shots, sources,
+// receivers and nt) stepped together: one launch per step covers every tile
+// of every shot of every instance still running.  Instances are ordered by
+// nt, longest first, so the running ones are a prefix; block b finds its
+// instance by binary search in the prefix sums of the per-instance block
+// counts, copies that instance's step arguments into shared memory and runs
+// the register-window step body on its tile.
+
+struct MultiInst {
+    StepArgs a[2];  // arguments with the ping-pong halves in order (cur = 0 / 1)
+    int tiles_z, tiles_x, nshots, nt;
+};
+
+template <int MODE, int TX>
+__global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 3)
+    step_kernel_multi(const MultiInst *inst, const int *prefix, int nactive, int it, int cur) {
+    extern __shared__ __align__(128) float smem[];
+    __shared__ StepArgs sa;
+    __shared__ int sinfo[4];
+    if (threadIdx.x == 0) {
+        const int b = blockIdx.x;
+        int lo = 0, hi = nactive - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (prefix[mid] <= b) lo = mid;
+            else hi = mid - 1;
+        }
+        const MultiInst &m = inst[lo];
+        const int local = b - prefix[lo], per_shot = m.tiles_z * m.tiles_x;
+        const int shot = local / per_shot, r = local - shot * per_shot;
+        const int xt = r / m.tiles_z, zt = r - xt * m.tiles_z;
+        sinfo[0] = lo;
+        sinfo[1] = shot;
+        sinfo[2] = xt * TX;
+        sinfo[3] = zt * 32;
+    }
+    __syncthreads();
+    const int *src = reinterpret_cast<const int *>(&inst[sinfo[0]].a[cur]);
+    int *dst = reinterpret_cast<int *>(&sa);
+    for (int w = threadIdx.x; w < (int)(sizeof(StepArgs) / 4); w += kThreads) dst[w] = src[w];
+    __syncthreads();
+    if (threadIdx.x == 0) sa.it = it;
+    __syncthreads();
+    const TmaMaps &unused = *reinterpret_cast<const TmaMaps *>(inst);  // the cp.async body never reads it
+    rw_body<MODE, TX, false>(sa, unused, smem, sinfo[2], sinfo[3], sinfo[1]);
 }
 
 // ------------------------------------------------ exact discrete adjoint
@@ -1152,6 +1211,152 @@ int launch_step(const fwi_batch *b, int adjoint, int it, bool snap_u_next, int s
         case FWI_SPIN: return launch_mode<FWI_SPIN>(a, b->nshots, b->tile, st);
     }
     return set_error(FWI_EINVAL, "unknown mode %d", b->mode);
+}
+
+// ---------------------------------------------- multi-instance host side
+
+// Forward step arguments of batch b for ping-pong half `cur` (no snapshots,
+// no segment stores).
+static void forward_args(const fwi_batch *b, int cur, StepArgs &a) {
+    base_args(b, a);
+    a.it = 0;
+    const int ns = nfields_sig(b->mode), nv = nfields_vel(b->mode), nxt = 1 - cur;
+    for (int f = 0; f < 6; f++) {
+        a.sig_in[f] = f < ns ? b->sig[cur][f] : nullptr;
+        a.sig_out[f] = f < ns ? b->sig[nxt][f] : nullptr;
+    }
+    for (int q = 0; q < 3; q++) {
+        const bool on = q < nv;
+        a.vel_in[q] = on ? b->vel[cur][q] : nullptr;
+        a.vel_out[q] = on ? b->vel[nxt][q] : nullptr;
+        a.disp[q] = on ? b->disp[q] : nullptr;
+        a.obs[q] = on ? b->obs[comp_slot(b->mode, q)] : nullptr;
+        a.snap_u[q] = a.snap_v[q] = a.seg_v[q] = a.seg_ds[q] = nullptr;
+    }
+    if (b->mode == FWI_SH) {
+        a.stf[0] = b->stf[1];
+        a.stf[1] = nullptr;
+    } else {
+        a.stf[0] = b->stf[0];
+        a.stf[1] = b->stf[2];
+    }
+}
+
+// Instances ordered by nt, longest first (stable), and the prefix sums of
+// their block counts.
+static void multi_plan(fwi_batch *const *bs, int n, int tx, int *order, long long *prefix) {
+    for (int i = 0; i < n; i++) order[i] = i;
+    for (int i = 1; i < n; i++)
+        for (int j = i; j > 0 && bs[order[j]]->nt > bs[order[j - 1]]->nt; j--) {
+            const int t = order[j];
+            order[j] = order[j - 1];
+            order[j - 1] = t;
+        }
+    prefix[0] = 0;
+    for (int i = 0; i < n; i++) {
+        const fwi_batch *b = bs[order[i]];
+        prefix[i + 1] = prefix[i] + (long long)((b->nz + 31) / 32) * ((b->nx + tx - 1) / tx) * b->nshots;
+    }
+}
+
+static int multi_tx(int tile) { return tile == 0 ? 32 : (tile_kind(tile) >= 1 && kTiles[tile].tz == 32 ? kTiles[tile].tx : -1); }
+
+long long multi_workspace_bytes(int n) {
+    return (long long)n * (long long)sizeof(MultiInst) + 4ll * (n + 1) + 256;
+}
+
+int multi_prepare(fwi_batch *const *bs, int n, void *ws, int (*check)(const fwi_batch *, int, int, int)) {
+    if (n < 1 || n > 4096 || !bs || !ws) return set_error(FWI_EINVAL, "fwi_multi_prepare: 1 <= n <= 4096 batches");
+    const int mode = bs[0]->mode, tx = multi_tx(bs[0]->tile);
+    if (tx < 0) return set_error(FWI_EINVAL, "fwi_multi_prepare: tile %d is not a 32-column register-window variant",
+                                 bs[0]->tile);
+    for (int i = 0; i < n; i++) {
+        int rc = check(bs[i], 0, 0, 0);
+        if (rc) return rc;
+        if (bs[i]->mode != mode || bs[i]->tile != bs[0]->tile)
+            return set_error(FWI_EINVAL, "fwi_multi_prepare: all batches need the same mode and tile");
+        if (bs[i]->cur != bs[0]->cur) return set_error(FWI_EINVAL, "fwi_multi_prepare: batches out of step (cur)");
+    }
+    int *order = new int[n];
+    long long *prefix = new long long[n + 1];
+    multi_plan(bs, n, tx, order, prefix);
+    if (prefix[n] >= (1ll << 31)) {
+        delete[] order;
+        delete[] prefix;
+        return set_error(FWI_ERANGE, "fwi_multi_prepare: %lld blocks per step exceed 2^31", prefix[n]);
+    }
+    MultiInst *h = new MultiInst[n];
+    int *hp = new int[n + 1];
+    for (int i = 0; i < n; i++) {
+        const fwi_batch *b = bs[order[i]];
+        forward_args(b, 0, h[i].a[0]);
+        forward_args(b, 1, h[i].a[1]);
+        h[i].tiles_z = (b->nz + 31) / 32;
+        h[i].tiles_x = (b->nx + tx - 1) / tx;
+        h[i].nshots = b->nshots;
+        h[i].nt = b->nt;
+    }
+    for (int i = 0; i <= n; i++) hp[i] = (int)prefix[i];
+    char *w = static_cast<char *>(ws);
+    cudaError_t e = cudaMemcpy(w, h, sizeof(MultiInst) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(w + sizeof(MultiInst) * n, hp, 4 * (n + 1), cudaMemcpyHostToDevice);
+    delete[] h;
+    delete[] hp;
+    delete[] order;
+    delete[] prefix;
+    (void)mode;
+    if (e != cudaSuccess) return set_error(FWI_ECUDA, "fwi_multi_prepare: %s", cudaGetErrorString(e));
+    return 0;
+}
+
+template <int MODE, int TX>
+static int launch_multi(const MultiInst *inst, const int *prefix, int nactive, int blocks, int it, int cur,
+                        cudaStream_t st) {
+    using T = Tile<MODE, TX, 32>;
+    static bool set = false;
+    if (!set) {
+        cudaError_t e = cudaFuncSetAttribute(step_kernel_multi<MODE, TX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)T::bytes);
+        if (e != cudaSuccess) return set_error(FWI_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+        set = true;
+    }
+    step_kernel_multi<MODE, TX><<<blocks, kThreads, T::bytes, st>>>(inst, prefix, nactive, it, cur);
+    return check_launch("step_kernel_multi");
+}
+
+int multi_run(fwi_batch *const *bs, int n, void *ws, int it0, int nsteps, cudaStream_t st) {
+    if (n < 1 || !bs || !ws || nsteps < 0 || it0 < 0) return set_error(FWI_EINVAL, "fwi_multi_run: bad arguments");
+    const int mode = bs[0]->mode, tx = multi_tx(bs[0]->tile);
+    if (tx != 32 && tx != 16 && tx != 64) return set_error(FWI_EINVAL, "fwi_multi_run: unsupported tile");
+    int *order = new int[n];
+    long long *prefix = new long long[n + 1];
+    multi_plan(bs, n, tx, order, prefix);
+    const MultiInst *inst = static_cast<const MultiInst *>(ws);
+    const int *pdev = reinterpret_cast<const int *>(static_cast<const char *>(ws) + sizeof(MultiInst) * n);
+    int rc = 0;
+    const int cur0 = bs[order[0]]->cur;
+    for (int it = it0; it < it0 + nsteps && !rc; it++) {
+        int nactive = 0;
+        while (nactive < n && bs[order[nactive]]->nt > it) nactive++;
+        if (!nactive) break;
+        const int cur = (cur0 + (it - it0)) & 1;
+        const int blocks = (int)prefix[nactive];
+        if (mode == FWI_SH) {
+            rc = tx == 32 ? launch_multi<FWI_SH, 32>(inst, pdev, nactive, blocks, it, cur, st)
+                 : tx == 16 ? launch_multi<FWI_SH, 16>(inst, pdev, nactive, blocks, it, cur, st)
+                            : launch_multi<FWI_SH, 64>(inst, pdev, nactive, blocks, it, cur, st);
+        } else if (mode == FWI_PSV) {
+            rc = tx == 32 ? launch_multi<FWI_PSV, 32>(inst, pdev, nactive, blocks, it, cur, st)
+                 : tx == 16 ? launch_multi<FWI_PSV, 16>(inst, pdev, nactive, blocks, it, cur, st)
+                            : launch_multi<FWI_PSV, 64>(inst, pdev, nactive, blocks, it, cur, st);
+        } else {
+            rc = launch_multi<FWI_SPIN, 32>(inst, pdev, nactive, blocks, it, cur, st);
+        }
+        for (int i = 0; i < nactive && !rc; i++) bs[order[i]]->cur ^= 1;
+    }
+    delete[] order;
+    delete[] prefix;
+    return rc;
 }
 
 }  // namespace fwi
