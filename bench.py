@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--profile-case", action="store_true",
                     help="only run a few forward steps (for ncu captures of the step kernel)")
     ap.add_argument("--autotune", action="store_true", help="time every tile variant and report the best")
+    ap.add_argument("--gradient", default="exact", choices=["exact", "reference"],
+                    help="exact: discrete adjoint with checkpointing (the solver's P-SV gradient); "
+                         "reference: snapshot-correlation adjoint of the reference's algorithm")
     return ap.parse_args()
 
 
@@ -89,7 +92,7 @@ def config_of(a, w, extra=None):
          "grid": [a.nx, a.nz], "shots": a.shots, "receivers": a.nrec, "nt": a.nt, "adjoint_interval": a.sae,
          "smooth_sigma": a.sigma, "cells_per_step": 2 * a.shots * a.nx * a.nz * a.nt,
          "l2": "inputs larger than L2 (wavefields of all shots and the snapshots exceed 126 MB); no flush",
-         "parallelism": "shots"}
+         "parallelism": "shots", "gradient": a.gradient}
     if extra:
         c.update(extra)
     return c
@@ -256,41 +259,66 @@ def main():
     data = [bt.obs[0].clone(), None, bt.obs[2].clone()]
     del bt
 
-    nsa = nt // a.sae
-    b = ShotBatch(m_init, nshots, nt, rid, sae=a.sae, nsa=nsa, snapshots=True, tile=a.tile)
-    k_lam = torch.zeros((nx, m_init.grid.pitch), dtype=torch.float64, device=dev)
-    k_mu = torch.zeros_like(k_lam)
-    adstf = [torch.empty(nshots * a.nrec * nt, dtype=torch.float32, device=dev) if c != 1 else None
-             for c in range(3)]
-    fwd = b.desc(inj=inj, stf=stf)
-    adj = b.desc(inj=adjoint_injection_lists(nshots, rid), stf=adstf, record=False, kernels=(k_lam, k_mu, None))
     stream = torch.cuda.current_stream()
-
     ev = {}
+    if a.gradient == "exact":
+        # exact discrete adjoint with checkpointed recomputation (the P-SV gradient of the solver)
+        from seispie_b200.adjoint import ExactAdjoint
+        ea = ExactAdjoint(m_init, nt, sid, lambda s: s, nshots, stf, rid, tile=a.tile)
+        grads = [torch.empty((nshots, a.nrec, nt), dtype=torch.float32, device=dev) if c != 1 else None
+                 for c in range(3)]
+        b = ea.fwd
+        fwd = ea.fdesc
+        adj = fwd
 
-    def gradient(record=False):
-        k_lam.zero_()
-        k_mu.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e2 = torch.cuda.Event(enable_timing=True)
-        e3 = torch.cuda.Event(enable_timing=True)
-        b.clear()
-        e0.record(stream)
-        b.run(fwd, False, 0, nt)
-        e1.record(stream)
-        mis = [engine.misfit(data[c], b.obs[c], adstf[c], nshots, a.nrec, nt, dt) for c in (0, 2)]
-        b.clear()
-        e2.record(stream)
-        b.run(adj, True, 0, nt)
-        e3.record(stream)
-        g = engine.smooth(k_mu, m_init.grid, a.sigma)
-        if world > 1:
-            dist.all_reduce(k_mu)
-        if record:
-            ev.setdefault("fwd", []).append((e0, e1))
-            ev.setdefault("adj", []).append((e2, e3))
-        return mis, g
+        def gradient(record=False):
+            e0, e1, e2, e3 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
+            e0.record(stream)
+            tr = ea.forward()
+            e1.record(stream)
+            mis = [engine.misfit_tracegrad(data[c], tr[c].reshape(-1), grads[c], nshots, a.nrec, nt, dt)
+                   for c in (0, 2)]
+            e2.record(stream)
+            k_lam, k_mu, k_buo = ea.backward(grads)
+            e3.record(stream)
+            g = engine.smooth(k_mu, m_init.grid, a.sigma)
+            if world > 1:
+                dist.all_reduce(k_mu)
+            if record:
+                ev.setdefault("fwd", []).append((e0, e1))
+                ev.setdefault("adj", []).append((e2, e3))
+            return mis, g
+    else:
+        nsa = nt // a.sae
+        b = ShotBatch(m_init, nshots, nt, rid, sae=a.sae, nsa=nsa, snapshots=True, tile=a.tile)
+        k_lam = torch.zeros((nx, m_init.grid.pitch), dtype=torch.float64, device=dev)
+        k_mu = torch.zeros_like(k_lam)
+        adstf = [torch.empty(nshots * a.nrec * nt, dtype=torch.float32, device=dev) if c != 1 else None
+                 for c in range(3)]
+        fwd = b.desc(inj=inj, stf=stf)
+        adj = b.desc(inj=adjoint_injection_lists(nshots, rid), stf=adstf, record=False,
+                     kernels=(k_lam, k_mu, None))
+
+        def gradient(record=False):
+            k_lam.zero_()
+            k_mu.zero_()
+            e0, e1, e2, e3 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
+            b.clear()
+            e0.record(stream)
+            b.run(fwd, False, 0, nt)
+            e1.record(stream)
+            mis = [engine.misfit(data[c], b.obs[c], adstf[c], nshots, a.nrec, nt, dt) for c in (0, 2)]
+            b.clear()
+            e2.record(stream)
+            b.run(adj, True, 0, nt)
+            e3.record(stream)
+            g = engine.smooth(k_mu, m_init.grid, a.sigma)
+            if world > 1:
+                dist.all_reduce(k_mu)
+            if record:
+                ev.setdefault("fwd", []).append((e0, e1))
+                ev.setdefault("adj", []).append((e2, e3))
+            return mis, g
 
     def tune():
         from seispie_b200.autotune import autotune
@@ -350,6 +378,7 @@ def main():
             "adjoint_step_us": adj_ms * 1e3 / nt}
     misfit_total = float(sum(m.sum().item() for m in mis))
     del b, fwd, adj
+    ea = grads = None  # noqa: F841  (release the checkpoint buffers before the e2e run)
     torch.cuda.empty_cache()
 
     # ----------------------------------------------------------------- e2e

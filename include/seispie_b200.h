@@ -214,6 +214,14 @@ int fwi_misfit(const float *data, const float *syn, float *adstf, double *misfit
                double *partial, int nshots, int nrec, int nt, double dt, void *stream);
 long long fwi_misfit_partials(int nrec, int nt);
 
+/* fwi_misfit writing, instead of the time-reversed adjoint source, the
+ * derivative of chi = sum taper^2 (syn - data)^2 with respect to every trace
+ * sample, in forward time order: grad = 2 taper^2 (syn - data) -- the input
+ * of fwi_run_transposed.  misfit[shot] is the same norm as fwi_misfit's.
+ * Same taper as waveform.py:11-21. */
+int fwi_misfit_tracegrad(const float *data, const float *syn, float *grad, double *misfit, double *partial,
+                         int nshots, int nrec, int nt, double dt, void *stream);
+
 /* Optimizer vector kernels (float32 vectors of n elements, FP64 arithmetic).
  * fwi_dot: *out = sum x[i]*y[i] in FP64, deterministic; partial is caller
  *   scratch of fwi_reduce_partials() doubles.  Replaces np.dot of

@@ -82,6 +82,8 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
                        ctypes.c_int),
         "fwi_misfit_partials": ([ctypes.c_int, ctypes.c_int], ctypes.c_longlong),
         "fwi_reduce_partials": ([], ctypes.c_longlong),
+        "fwi_misfit_tracegrad": ([_vp, _vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                  _vp], ctypes.c_int),
         "fwi_dot": ([_vp, _vp, ctypes.c_longlong, _vp, _vp, _vp], ctypes.c_int),
         "fwi_absmax": ([_vp, ctypes.c_longlong, _vp, _vp, _vp], ctypes.c_int),
         "fwi_axpby": ([_vp, ctypes.c_double, _vp, ctypes.c_double, _vp, ctypes.c_longlong, _vp], ctypes.c_int),

@@ -185,6 +185,11 @@ constexpr int kMisfitBlock = 256;
 // diff, waveform.py:5-25.  One thread per (shot, receiver, sample).  The
 // Hann-taper weight is computed in double and rounded to float before use,
 // as the float32 arithmetic of the reference does.
+// GRAD = true writes, instead of the time-reversed adjoint source, the
+// derivative of chi = sum taper^2 (syn - data)^2 with respect to each trace
+// sample in forward time order: 2 taper^2 (syn - data) = -adstf reversed
+// (the input of the exact adjoint, fwi_run_transposed).
+template <bool GRAD>
 __global__ void misfit_kernel(const float *data, const float *syn, float *adstf, double *partial, int nrec, int nt,
                               double dt) {
     __shared__ double red[kMisfitBlock / 32];
@@ -199,7 +204,9 @@ __global__ void misfit_kernel(const float *data, const float *syn, float *adstf,
         const float tp = (float)taper;
         const long long kt = row * nt + it;
         const float r = __fmul_rn(__fsub_rn(data[kt], syn[kt]), tp);
-        adstf[row * nt + nt - it - 1] = __fmul_rn(__fmul_rn(r, tp), 2.f);
+        const float a = __fmul_rn(__fmul_rn(r, tp), 2.f);
+        if (GRAD) adstf[kt] = -a;
+        else adstf[row * nt + nt - it - 1] = a;
         sq = (double)r * (double)r;
     }
     for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
@@ -230,9 +237,10 @@ __global__ void misfit_finish_kernel(const double *partial, double *misfit, long
 long long misfit_partials(int nrec, int nt) { return (long long)nrec * ((nt + kMisfitBlock - 1) / kMisfitBlock); }
 
 int launch_misfit(const float *data, const float *syn, float *adstf, double *misfit, double *partial, int nshots,
-                  int nrec, int nt, double dt, cudaStream_t st) {
+                  int nrec, int nt, double dt, cudaStream_t st, bool grad) {
     dim3 grid((nt + kMisfitBlock - 1) / kMisfitBlock, nrec, nshots);
-    misfit_kernel<<<grid, kMisfitBlock, 0, st>>>(data, syn, adstf, partial, nrec, nt, dt);
+    if (grad) misfit_kernel<true><<<grid, kMisfitBlock, 0, st>>>(data, syn, adstf, partial, nrec, nt, dt);
+    else misfit_kernel<false><<<grid, kMisfitBlock, 0, st>>>(data, syn, adstf, partial, nrec, nt, dt);
     int rc = check_launch("misfit");
     if (rc) return rc;
     misfit_finish_kernel<<<nshots, 256, 0, st>>>(partial, misfit, misfit_partials(nrec, nt));

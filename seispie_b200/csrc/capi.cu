@@ -40,7 +40,7 @@ long long multi_workspace_bytes(int n);
 int multi_prepare(fwi_batch *const *bs, int n, void *ws, int (*check)(const fwi_batch *, int, int, int));
 int multi_run(fwi_batch *const *bs, int n, void *ws, int it0, int nsteps, cudaStream_t st);
 int launch_misfit(const float *data, const float *syn, float *adstf, double *misfit, double *partial, int nshots,
-                  int nrec, int nt, double dt, cudaStream_t st);
+                  int nrec, int nt, double dt, cudaStream_t st, bool grad);
 long long misfit_partials(int nrec, int nt);
 int launch_smooth(const double *in, int in_pitch, float *out, int out_pitch, double *tmp, int nx, int nz, int sigma,
                   cudaStream_t st);
@@ -270,7 +270,15 @@ int fwi_misfit(const float *data, const float *syn, float *adstf, double *misfit
         cudaError_t e = cudaMemsetAsync(misfit, 0, sizeof(double) * nshots, (cudaStream_t)stream);
         return e == cudaSuccess ? 0 : set_error(FWI_ECUDA, "fwi_misfit: %s", cudaGetErrorString(e));
     }
-    return launch_misfit(data, syn, adstf, misfit, partial, nshots, nrec, nt, dt, (cudaStream_t)stream);
+    return launch_misfit(data, syn, adstf, misfit, partial, nshots, nrec, nt, dt, (cudaStream_t)stream, false);
+}
+
+int fwi_misfit_tracegrad(const float *data, const float *syn, float *grad, double *misfit, double *partial,
+                         int nshots, int nrec, int nt, double dt, void *stream) {
+    REQUIRE(data && syn && grad && misfit && partial, "fwi_misfit_tracegrad: NULL pointer");
+    REQUIRE(nshots >= 1 && nshots <= 65535 && nrec >= 1 && nrec <= 65535 && nt >= 1,
+            "fwi_misfit_tracegrad: nshots in [1, 65535], nrec in [1, 65535], nt >= 1");
+    return launch_misfit(data, syn, grad, misfit, partial, nshots, nrec, nt, dt, (cudaStream_t)stream, true);
 }
 
 int fwi_smooth(const double *in, int in_pitch, float *out, int out_pitch, double *tmp, int nx, int nz, int sigma,

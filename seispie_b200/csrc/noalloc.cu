@@ -24,7 +24,7 @@
 namespace fwi {
 
 int launch_misfit(const float *data, const float *syn, float *adstf, double *misfit, double *partial, int nshots,
-                  int nrec, int nt, double dt, cudaStream_t st);
+                  int nrec, int nt, double dt, cudaStream_t st, bool grad);
 long long misfit_partials(int nrec, int nt);
 
 static __device__ __align__(256) double g_misfit_scratch[FWI_MISFIT_NOALLOC_MAX_PARTIALS];
@@ -73,5 +73,5 @@ extern "C" int fwi_misfit_noalloc(const float *data, const float *syn, float *ad
     double *scratch = nullptr;
     int rc = misfit_scratch(&scratch);
     if (rc) return rc;
-    return launch_misfit(data, syn, adstf, misfit, scratch, nshots, nrec, nt, dt, (cudaStream_t)stream);
+    return launch_misfit(data, syn, adstf, misfit, scratch, nshots, nrec, nt, dt, (cudaStream_t)stream, false);
 }

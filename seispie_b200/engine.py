@@ -315,6 +315,18 @@ def misfit(data: torch.Tensor, syn: torch.Tensor, adstf: torch.Tensor, nshots: i
     return out
 
 
+def misfit_tracegrad(data: torch.Tensor, syn: torch.Tensor, grad: torch.Tensor, nshots: int, nrec: int, nt: int,
+                     dt: float, stream=None) -> torch.Tensor:
+    """Per-shot misfit norm (FP64) and dchi/dsyn in forward time order
+    (fwi_misfit_tracegrad)."""
+    lib = _lib.load()
+    out = torch.zeros(nshots, dtype=torch.float64, device=data.device)
+    part = torch.zeros(max(1, nshots * lib.fwi_misfit_partials(nrec, nt)), dtype=torch.float64, device=data.device)
+    check(lib.fwi_misfit_tracegrad(ptr(data), ptr(syn), ptr(grad), ptr(out), ptr(part), nshots, nrec, nt, float(dt),
+                                   stream_handle(stream)), "fwi_misfit_tracegrad")
+    return out
+
+
 def smooth(k: torch.Tensor, grid: Grid, sigma: int, stream=None) -> torch.Tensor:
     """Gaussian smoothing of an FP64 [nx, pitch] kernel into float32 [npt]."""
     out = torch.empty(grid.npt, dtype=torch.float32, device=k.device)

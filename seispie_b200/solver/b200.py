@@ -233,9 +233,54 @@ class b200:
         field = g.nx * g.pitch * 4
         ns, nv = engine.NS[mode], engine.NV[mode]
         b = (2 * ns + 3 * nv) * field + 4 * self.nrec * self.nt * nv * 3
+        if snapshots and self._exact(mode):
+            from ..adjoint import default_segment
+            k = default_segment(self.nt, mode, 1, g)
+            # checkpoints, segment stores, and the adjoint's own wavefields
+            return b + (-(-self.nt // k) * (ns + 2 * nv) + k * 2 * nv + 2 * ns + 3 * nv) * field
         if snapshots:
             b += self.nsa * min(nv, 2) * field * (2 if (mode != FWI_SH and self.kernel_rho) else 1)
         return b
+
+    def _exact(self, mode) -> bool:
+        """Gradient by the exact discrete adjoint?  Default: yes for P-SV (the
+        reference's P-SV adjoint cannot run, solver.py:324-329), no for SH
+        (its continuous-adjoint kernel equals dt times the exact gradient)."""
+        g = self.config.get("gradient", "")
+        if g in ("exact", "reference"):
+            return g == "exact" and mode in (FWI_SH, FWI_PSV)
+        return mode == FWI_PSV
+
+    def _exact_gradient(self, mode, shots, data_of) -> float:
+        """Misfit and exact gradient of this process's shots, accumulated in
+        the reference's units (dt * dchi/dparam) into k_lam_f64 / k_mu_f64 /
+        k_rho_f64; returns the misfit (sum of per-shot, per-component norms)."""
+        from ..adjoint import ExactAdjoint
+        combine = self.config["combine_sources"] == "yes"
+        misfit = 0.0
+        nrec, nt = self.nrec, self.nt
+        for chunk in self._chunks(shots, mode, True):
+            n = len(chunk)
+            with self._ctx():
+                ea = ExactAdjoint(self.model, nt, self.src_id, lambda s: -1 if combine else chunk[s], n,
+                                  self._stf(mode), self.rec_id, tile=self.tile)
+                tr = ea.forward()
+                grads = [None, None, None]
+                for c, lst in data_of:
+                    data = torch.from_numpy(np.stack([lst[shots.index(i)] for i in chunk]))
+                    data = data.pin_memory().to(self.device, non_blocking=True)
+                    grads[c] = torch.empty(n * nrec * nt, dtype=torch.float32, device=self.device)
+                    syn = tr[c].reshape(-1).contiguous()
+                    misfit += float(engine.misfit_tracegrad(data, syn, grads[c], n, nrec, nt, self.dt).sum().item())
+                    grads[c] = grads[c].view(n, nrec, nt)
+                k_lam, k_mu, k_buo = ea.backward(grads)
+                self.k_lam_f64 += self.dt * k_lam
+                self.k_mu_f64 += self.dt * k_mu
+                # buo = dt/rho: dchi/drho = -dchi/dbuo * dt / rho^2
+                rho = self.model.rho.double()
+                self.k_rho_f64 -= self.dt * k_buo * self.dt / torch.where(rho > 0, rho * rho, torch.ones_like(rho))
+                del ea
+        return misfit
 
     def _max_batch(self, mode, snapshots):
         budget = self.batch_memory
@@ -401,6 +446,9 @@ class b200:
                    FWI_SPIN: [(0, self.syn_x), (2, self.syn_z)]}
         for mode in self.modes:
             snapv = adj and mode != FWI_SH and self.kernel_rho
+            if adj and self._exact(mode):
+                misfit += self._exact_gradient(mode, shots, data_of[mode])
+                continue
             for chunk in self._chunks(shots, mode, adj):
                 b = self._forward_batch(mode, chunk, snapshots=bool(adj), snap_velocity=snapv)
                 n, nrec, nt = len(chunk), self.nrec, self.nt

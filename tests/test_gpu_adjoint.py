@@ -152,3 +152,65 @@ def test_autograd_through_vp_vs_rho():
 
     fd = (chi_of(vs + eps * d) - chi_of(vs - eps * d)) / (2 * eps)
     assert abs(float((gvs * d).sum()) - fd) < 1e-3 * abs(fd)
+
+
+def test_misfit_tracegrad_is_reversed_negated_adjoint_source():
+    from seispie_b200 import engine
+    rng = np.random.default_rng(4)
+    ns, nrec, nt = 2, 5, 333
+    d = torch.as_tensor(rng.standard_normal(ns * nrec * nt).astype(np.float32)).cuda()
+    s = torch.as_tensor(rng.standard_normal(ns * nrec * nt).astype(np.float32)).cuda()
+    ad, g = torch.empty_like(d), torch.empty_like(d)
+    m1 = engine.misfit(d, s, ad, ns, nrec, nt, 2e-3)
+    m2 = engine.misfit_tracegrad(d, s, g, ns, nrec, nt, 2e-3)
+    assert torch.equal(m1, m2)
+    assert torch.equal(g.view(ns, nrec, nt), -ad.view(ns, nrec, nt).flip(-1))
+
+
+def test_plugin_psv_gradient_is_dt_times_exact(tmp_path):
+    """compute_gradient of the b200 plugin for P-SV (exact adjoint by
+    default) equals dt times the autograd gradient, before smoothing."""
+    import os
+    from seispie_b200.adjoint import AcquisitionSetup, Seismograms, waveform_misfit
+    from seispie_b200.engine import Grid
+    from seispie_b200.io import write_model
+    from seispie_b200.solver import b200
+    nx, nz, h, nt = 44, 38, 10.0, 240
+    i, j = np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij")
+    vs_true = 1732 * (1 + 0.05 * np.sign(np.sin(i / 5.0) * np.sin(j / 5.0) + 1e-9))
+    root = str(tmp_path)
+    for d, vs in (("true", vs_true.ravel()), ("init", np.full(nx * nz, 1732.0))):
+        write_model(os.path.join(root, d), nx, nz, h, h, dict(vp=np.full(nx * nz, 3000.0), vs=vs,
+                                                              rho=np.full(nx * nz, 2600.0)))
+    src = np.array([[100.0, 60.0, 0, 14.0, 0.07, 20.0, 1e10], [300.0, 60.0, 0, 14.0, 0.07, -30.0, 1e10]])
+    rec = np.array([[30.0 + 30 * r, 80.0] for r in range(12)])
+    np.savetxt(os.path.join(root, "src.dat"), src)
+    np.savetxt(os.path.join(root, "rec.dat"), rec)
+    os.makedirs(os.path.join(root, "out"))
+    s = b200()
+    s.config = dict(nt=str(nt), dt="1e-3", sh="no", psv="yes", abs_left="yes", abs_right="yes", abs_top="no",
+                    abs_bottom="yes", abs_width="8", abs_alpha="0.05", save_coordinates="", combine_sources="no",
+                    save_snapshot="0", adjoint_interval="4", smooth="2")
+    s.path = dict(model_true=os.path.join(root, "true"), model_init=os.path.join(root, "init"),
+                  sources=os.path.join(root, "src.dat"), stations=os.path.join(root, "rec.dat"),
+                  output=os.path.join(root, "out"))
+    s.mpi = None
+    s.setup(None)
+    s.import_model(1)
+    s.import_sources()
+    s.import_stations()
+    s.import_traces()
+    s.import_model(0)
+    s.compute_gradient()
+    kraw = s.k_mu_f64[:, :nz].cpu().numpy()
+    setup = AcquisitionSetup("psv", Grid(nx, nz, h, h), 1e-3, nt, src, rec, (8, 0.05, 1, 1, 1, 0))
+    rho = torch.full((nx, nz), 2600.0, device="cuda")
+    vp = torch.full((nx, nz), 3000.0, device="cuda")
+    lam = rho * (vp * vp - 2 * 1732.0 ** 2)
+    mu = (rho * 1732.0 ** 2).clone().requires_grad_(True)
+    data = torch.stack([torch.as_tensor(np.stack(s.syn_x)).view(2, 12, nt),
+                        torch.as_tensor(np.stack(s.syn_z)).view(2, 12, nt)]).cuda()
+    chi = waveform_misfit(Seismograms.apply(lam, mu, rho, setup), data, setup.dt)
+    chi.backward()
+    ref = 1e-3 * mu.grad.double().cpu().numpy()
+    assert np.linalg.norm(kraw - ref) / np.linalg.norm(ref) < 1e-5
