@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define FWI_ABI_VERSION 2
+#define FWI_ABI_VERSION 3
 
 /* status codes */
 #define FWI_OK 0
@@ -190,17 +190,19 @@ int fwi_multi_run(fwi_batch *const *batches, int n, void *workspace, int it0, in
 
 /* Exact discrete adjoint of fwi_run's SH / P-SV forward step, run backwards
  * over forward steps it = it_hi-1 down to it_hi-nsteps on the adjoint state
- * held in the batch's wavefield buffers (sig~, v~, u~; cleared by the caller
- * before the last step).  Before transposing step it, the trace gradients
- * stf_c[inj_row[e]*nt + it] (dL/d trace in forward time order; rows as for
- * fwi_run's injection, typically one per receiver and shot) are added to u~
- * at inj_cell[e].  Each step also accumulates, over every shot, into the FP64
- * arrays: dL/dlam (k_lam, P-SV), dL/dmu (k_mu), dL/dbuo with buo = dt/rho
- * (k_rho).  Needs the forward v(it+1) and divergence of step it in seg_v /
- * seg_ds for every step of the range (written by a forward fwi_run over the
- * same segment).  No counterpart in the reference, whose adjoint
- * (solver.py:290-329) is the continuous-adjoint approximation fwi_run's
- * adjoint = 1 reproduces. */
+ * held in the batch's stress and velocity buffers (sig~, v~; cleared by the
+ * caller before the last step; disp is not used).  The adjoint displacement
+ * u~ is nonzero only at the receivers, where it is the suffix sum over the
+ * steps s >= it of dL/d trace(s): stf_c[inj_row[e]*nt + it] holds that value
+ * for entry e (fwi_trace_suffix_sum of the trace gradients; rows as for
+ * fwi_run's injection, typically one per receiver and shot) and enters v~ as
+ * dt * u~ at inj_cell[e].  Each step also accumulates, over every shot, into
+ * the FP64 arrays: dL/dlam (k_lam, P-SV), dL/dmu (k_mu), dL/dbuo with buo =
+ * dt/rho (k_rho); NULL skips an array.  Needs the forward v(it+1) and
+ * divergence of step it in seg_v / seg_ds for every step of the range
+ * (written by a forward fwi_run over the same segment).  No counterpart in
+ * the reference, whose adjoint (solver.py:290-329) is the continuous-adjoint
+ * approximation fwi_run's adjoint = 1 reproduces. */
 int fwi_run_transposed(fwi_batch *b, int it_hi, int nsteps, void *stream);
 
 /* L2 waveform misfit and adjoint source for nshots x nrec traces of nt
@@ -221,6 +223,12 @@ long long fwi_misfit_partials(int nrec, int nt);
  * Same taper as waveform.py:11-21. */
 int fwi_misfit_tracegrad(const float *data, const float *syn, float *grad, double *misfit, double *partial,
                          int nshots, int nrec, int nt, double dt, void *stream);
+
+/* Suffix sums along time of ntraces traces of nt samples ([trace][t]):
+ * out[t] = sum over s >= t of g[s], accumulated in FP64; out may alias g.
+ * Turns trace gradients (fwi_misfit_tracegrad) into the injection values of
+ * fwi_run_transposed. */
+int fwi_trace_suffix_sum(const float *g, float *out, long long ntraces, int nt, void *stream);
 
 /* Optimizer vector kernels (float32 vectors of n elements, FP64 arithmetic).
  * fwi_dot: *out = sum x[i]*y[i] in FP64, deterministic; partial is caller

@@ -13,7 +13,7 @@ from . import build as _build
 
 FWI_SH, FWI_PSV, FWI_SPIN = 0, 1, 2
 MODES = {"sh": FWI_SH, "psv": FWI_PSV, "spin": FWI_SPIN}
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 _fp = ctypes.POINTER(ctypes.c_float)
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -84,6 +84,7 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
         "fwi_reduce_partials": ([], ctypes.c_longlong),
         "fwi_misfit_tracegrad": ([_vp, _vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                   _vp], ctypes.c_int),
+        "fwi_trace_suffix_sum": ([_vp, _vp, ctypes.c_longlong, ctypes.c_int, _vp], ctypes.c_int),
         "fwi_dot": ([_vp, _vp, ctypes.c_longlong, _vp, _vp, _vp], ctypes.c_int),
         "fwi_absmax": ([_vp, ctypes.c_longlong, _vp, _vp, _vp], ctypes.c_int),
         "fwi_axpby": ([_vp, ctypes.c_double, _vp, ctypes.c_double, _vp, ctypes.c_longlong, _vp], ctypes.c_int),

@@ -87,7 +87,9 @@ class ExactAdjoint:
         stf = [None, None, None]
         for c in range(3):
             if g_traces[c] is not None and self.fwd.obs[c] is not None:
-                stf[c] = g_traces[c].reshape(-1).to(torch.float32).contiguous()
+                # u~ at the receivers: suffix sums of dL/d(trace) over time
+                g = g_traces[c].to(torch.float32).contiguous()
+                stf[c] = engine.trace_suffix_sum(g, torch.empty_like(g)).reshape(-1)
         adj = ShotBatch(self.model, self.nshots, self.nt, self.rec_id)
         adj.clear()
         inj = adjoint_injection_lists(self.nshots, self.rec_id) if len(self.rec_id) else None

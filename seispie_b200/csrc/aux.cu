@@ -247,6 +247,41 @@ int launch_misfit(const float *data, const float *syn, float *adstf, double *mis
     return check_launch("misfit_finish");
 }
 
+// Suffix sums along time of every trace: out[t] = sum_{s >= t} g[s], one CTA
+// per trace walking 256-sample chunks from the end; an FP64 scan inside each
+// chunk (warp shuffles, then the warp totals) plus the running carry, so the
+// result does not depend on the launch and out may alias g.
+__global__ void suffix_sum_kernel(const float *g, float *out, int nt) {
+    __shared__ double wsum[8];
+    const long long base = (long long)blockIdx.x * nt;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double carry = 0.0;
+    for (int end = nt; end > 0; end -= 256) {
+        const int t = end - 1 - tid;  // thread i holds the i-th sample counted from the end of the chunk
+        double v = t >= 0 ? (double)g[base + t] : 0.0;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const double u = __shfl_up_sync(0xffffffffu, v, d);
+            if (lane >= d) v += u;
+        }
+        if (lane == 31) wsum[warp] = v;
+        __syncthreads();
+        double before = carry, total = carry;
+        for (int w = 0; w < 8; w++) {
+            if (w < warp) before += wsum[w];
+            total += wsum[w];
+        }
+        if (t >= 0) out[base + t] = (float)(before + v);
+        carry = total;
+        __syncthreads();
+    }
+}
+
+int launch_suffix_sum(const float *g, float *out, long long ntraces, int nt, cudaStream_t st) {
+    suffix_sum_kernel<<<(unsigned)ntraces, 256, 0, st>>>(g, out, nt);
+    return check_launch("suffix_sum");
+}
+
 // ---------------------------------------------------------------- smoothing
 // init_gausian / apply_gauxxian_x / apply_gauxxian_z, fd2d.py:76-108.
 // gaussian(d) = exp(-d^2 / (2 sigma^2)) / (sqrt(2 pi) sigma), fd2d.py:71-73.

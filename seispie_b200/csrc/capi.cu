@@ -42,6 +42,7 @@ int multi_run(fwi_batch *const *bs, int n, void *ws, int it0, int nsteps, cudaSt
 int launch_misfit(const float *data, const float *syn, float *adstf, double *misfit, double *partial, int nshots,
                   int nrec, int nt, double dt, cudaStream_t st, bool grad);
 long long misfit_partials(int nrec, int nt);
+int launch_suffix_sum(const float *g, float *out, long long ntraces, int nt, cudaStream_t st);
 int launch_smooth(const double *in, int in_pitch, float *out, int out_pitch, double *tmp, int nx, int nz, int sigma,
                   cudaStream_t st);
 int launch_vps2lm(float *lam, float *mu, const float *rho, long long n, cudaStream_t st);
@@ -279,6 +280,13 @@ int fwi_misfit_tracegrad(const float *data, const float *syn, float *grad, doubl
     REQUIRE(nshots >= 1 && nshots <= 65535 && nrec >= 1 && nrec <= 65535 && nt >= 1,
             "fwi_misfit_tracegrad: nshots in [1, 65535], nrec in [1, 65535], nt >= 1");
     return launch_misfit(data, syn, grad, misfit, partial, nshots, nrec, nt, dt, (cudaStream_t)stream, true);
+}
+
+int fwi_trace_suffix_sum(const float *g, float *out, long long ntraces, int nt, void *stream) {
+    REQUIRE(g && out, "fwi_trace_suffix_sum: NULL pointer");
+    REQUIRE(ntraces >= 0 && ntraces <= 0x7fffffffll && nt >= 0, "fwi_trace_suffix_sum: ntraces in [0, 2^31), nt >= 0");
+    if (ntraces == 0 || nt == 0) return 0;
+    return launch_suffix_sum(g, out, ntraces, nt, (cudaStream_t)stream);
 }
 
 int fwi_smooth(const double *in, int in_pitch, float *out, int out_pitch, double *tmp, int nx, int nz, int sigma,

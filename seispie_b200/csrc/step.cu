@@ -35,9 +35,13 @@
 // Derivative masks follow solver.py:22-51 exactly: D- is zero unless
 // 2 <= i < n-2, D+ is zero unless 1 <= i < n-2 (same for j), so no value
 // outside the grid or in row padding ever reaches a result.
+#include <cooperative_groups.h>
+
 #include <cstdio>
 
 #include "common.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace fwi {
 
@@ -697,310 +701,6 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 3)
     rw_body<MODE, TX, false>(sa, unused, smem, sinfo[2], sinfo[3], sinfo[1]);
 }
 
-// ------------------------------------------------ exact discrete adjoint
-//
-// The forward step above is linear in the state.  For SH / P-SV it reads
-//   d  = D- sig + f            (stress divergence plus sources)
-//   v' = B (v + b d)           (b = dt/rho, B = sponge)
-//   u' = u + dt v'
-//   sig' = sig + dt S(D+ v')   (S: lam/mu stress-strain law)
-// Its exact transpose, run backwards in time on the adjoint state
-// (sig~, v~, u~), is one launch of adjoint_kernel per step:
-//   u~  += P^T g               (g = dL/d(trace) of this step, at receivers)
-//   a    = v~ + dt u~ + (D+)^T (dt S^T sig~)
-//   v~'  = B a
-//   sig~' = sig~ + (D-)^T (b v~')
-// with (D+)^T and (D-)^T the transposes of the reference's masked stencils
-// (solver.py:22-51) -- boundary masks included, so the adjoint is exact to
-// rounding.  grad_kernel then adds this step's terms of
-//   dL/dlam = sum dt (sxx~+szz~)(exx+ezz),
-//   dL/dmu  = sum dt (2 sxx~ exx + 2 szz~ ezz + sxz~ (exz+ezx))  [SH: dt (sxy~ exy + szy~ ezy)]
-//   dL/db   = sum v~' . d
-// from the forward v' and d stored per step by a recomputed forward segment.
-
-struct AdjArgs {
-    int nx, nz, pitch, nt, it;
-    FastDiv divnz;
-    float cx1, cx2, cz1, cz2, dt;
-    const float *sig_in[3];
-    float *sig_out[3];
-    const float *vel_in[2];
-    float *vel_out[2];
-    float *disp[2];
-    const float *buo, *bound, *lam, *mu;
-    const int *inj_ptr, *inj_cell, *inj_row;
-    const float *g[2];  // trace gradients in forward time order, injected into u~
-};
-
-template <int MODE, int TX, int TZ>
-struct AdjTile {
-    using F = Fields<MODE>;
-    static constexpr int SX = TX + 6, SZ = TZ + 8, VX = TX + 3, RVZ = TZ + 3;
-    static constexpr int NL = MODE == FWI_SH ? 1 : 2;   // stiffness fields staged with halo
-    static constexpr int NTT = MODE == FWI_SH ? 2 : 3;  // dt S^T sig~ fields
-    static constexpr int FS = (SX * SZ + 3) / 4 * 4, FV = (VX * SZ + 3) / 4 * 4;
-    static constexpr int S_SZ = (F::NS + NL + NTT) * FS;
-    static constexpr int V_SZ = (2 * F::NV + 2) * FV;
-    static constexpr int J_SZ = F::NINJ * VX * RVZ;
-    static constexpr int LIST = kThreads * (1 + F::NINJ) + 8;
-    static constexpr size_t bytes = sizeof(float) * (size_t)(S_SZ + V_SZ + J_SZ + LIST);
-};
-
-template <int MODE, int TX, int TZ>
-__global__ void __launch_bounds__(kThreads, 2) adjoint_kernel(const AdjArgs a) {
-    using T = AdjTile<MODE, TX, TZ>;
-    using F = Fields<MODE>;
-    constexpr int SX = T::SX, SZ = T::SZ, VX = T::VX, RVZ = T::RVZ, FS = T::FS, FV = T::FV;
-    constexpr int NS = F::NS, NV = F::NV, NL = T::NL;
-    extern __shared__ __align__(128) float smem[];
-    float *sSig = smem, *sL = sSig + NS * FS, *sT = sL + NL * FS;
-    float *sV = sT + T::NTT * FS, *sU = sV + NV * FV, *sB = sU + NV * FV;
-    float *sJ = sB + 2 * FV;
-    int *sLoc = reinterpret_cast<int *>(sJ + T::J_SZ);
-    float *sVal = reinterpret_cast<float *>(sLoc + kThreads);
-    int *sWarp = reinterpret_cast<int *>(sVal + F::NINJ * kThreads);
-
-    const int tid = threadIdx.x;
-    const int z0 = blockIdx.x * TZ, x0 = blockIdx.y * TX, shot = blockIdx.z;
-    const int nx = a.nx, nz = a.nz, pitch = a.pitch;
-    const long long soff = (long long)shot * nx * pitch;
-    const float *lm[2] = {MODE == FWI_SH ? a.mu : a.lam, a.mu};
-    const float *bb[2] = {a.buo, a.bound};
-    stage_strided<NS, SX, SZ, FS>(sSig, a.sig_in, soff, x0 - 3, z0 - 4, nx, pitch, tid);
-    stage_strided<NL, SX, SZ, FS>(sL, lm, 0, x0 - 3, z0 - 4, nx, pitch, tid);
-    stage_strided<NV, VX, SZ, FV>(sV, a.vel_in, soff, x0 - 1, z0 - 4, nx, pitch, tid);
-    stage_strided<NV, VX, SZ, FV>(sU, a.disp, soff, x0 - 1, z0 - 4, nx, pitch, tid);
-    stage_strided<2, VX, SZ, FV>(sB, bb, 0, x0 - 1, z0 - 4, nx, pitch, tid);
-    cp_async_commit();
-    const bool has_inj = scatter_entries<F::NINJ, VX, RVZ>(a.inj_ptr, a.inj_cell, a.inj_row, a.g, a.nt, a.it,
-                                                           a.divnz, nz, x0, z0, shot, sJ, sLoc, sVal, sWarp);
-    cp_async_wait_all();
-    __syncthreads();
-
-    const float dt = a.dt, cx1 = a.cx1, cx2 = a.cx2, cz1 = a.cz1, cz2 = a.cz2;
-    // t = dt S^T sig~ over the whole stress region (zero outside the grid)
-    for (int c = tid; c < SX * SZ; c += kThreads) {
-        if (MODE == FWI_SH) {
-            const float m = sL[c];
-            sT[c] = dt * (m * sSig[c]);
-            sT[FS + c] = dt * (m * sSig[FS + c]);
-        } else {
-            const float l = sL[c], m = sL[FS + c], l2m = l + 2.f * m;
-            const float sxx = sSig[c], szz = sSig[FS + c], sxz = sSig[2 * FS + c];
-            sT[c] = dt * (l2m * sxx + l * szz);
-            sT[FS + c] = dt * (l * sxx + l2m * szz);
-            sT[2 * FS + c] = dt * (m * sxz);
-        }
-    }
-    __syncthreads();
-
-    // velocity-like half on the computed region (rows x0-1..x0+TX+1, columns z0-1..z0+TZ+1)
-    auto mxp = [&](int k) -> float { return (k >= 1 && k < nx - 2) ? 1.f : 0.f; };
-    auto mzp = [&](int k) -> float { return (k >= 1 && k < nz - 2) ? 1.f : 0.f; };
-    for (int c = tid; c < VX * RVZ; c += kThreads) {
-        const int rx = c / RVZ, rz = c - rx * RVZ;
-        const int gx = x0 - 1 + rx, gz = z0 - 1 + rz;
-        const int vi = rx * SZ + rz + 3, si = (rx + 2) * SZ + rz + 3;
-        if (gx < 0 || gx >= nx || gz < 0 || gz >= nz) {
-#pragma unroll
-            for (int q = 0; q < NV; q++) sV[q * FV + vi] = 0.f;
-            continue;
-        }
-        // (D+)^T along x and z of field f of t
-        auto dxpT = [&](int f) -> float {
-            const float *t = sT + f * FS + si;
-            return cx1 * (t[-SZ] * mxp(gx - 1) - t[0] * mxp(gx)) - cx2 * (t[-2 * SZ] * mxp(gx - 2) - t[SZ] * mxp(gx + 1));
-        };
-        auto dzpT = [&](int f) -> float {
-            const float *t = sT + f * FS + si;
-            return cz1 * (t[-1] * mzp(gz - 1) - t[0] * mzp(gz)) - cz2 * (t[-2] * mzp(gz - 2) - t[1] * mzp(gz + 1));
-        };
-        float acc[2];
-        if (MODE == FWI_SH) {
-            acc[0] = dxpT(0) + dzpT(1);
-        } else {
-            acc[0] = dxpT(0) + dzpT(2);
-            acc[1] = dxpT(2) + dzpT(1);
-        }
-        const bool interior = rx >= 1 && rx <= TX && rz >= 1 && rz <= TZ;
-        const long long g = soff + (long long)gx * pitch + gz;
-        const float bnd = sB[FV + vi], buo = sB[vi];
-#pragma unroll
-        for (int q = 0; q < NV; q++) {
-            float uu = sU[q * FV + vi];
-            if (has_inj) uu += sJ[q * VX * RVZ + rx * RVZ + rz];
-            const float vn = bnd * ((sV[q * FV + vi] + dt * uu) + acc[q]);
-            sV[q * FV + vi] = buo * vn;  // b v~' for the stress-like half
-            if (interior) {
-                a.vel_out[q][g] = vn;
-                a.disp[q][g] = uu;
-            }
-        }
-    }
-    __syncthreads();
-
-    // stress-like half on the interior: sig~' = sig~ + (D-)^T (b v~')
-    auto mxm = [&](int k) -> float { return (k >= 2 && k < nx - 2) ? 1.f : 0.f; };
-    auto mzm = [&](int k) -> float { return (k >= 2 && k < nz - 2) ? 1.f : 0.f; };
-    for (int c = tid; c < TX * TZ; c += kThreads) {
-        const int ix = c / TZ, iz = c - ix * TZ;
-        const int gx = x0 + ix, gz = z0 + iz;
-        if (gx >= nx || gz >= nz) continue;
-        const int vi = (ix + 1) * SZ + iz + 4, si = (ix + 3) * SZ + iz + 4;
-        auto dxmT = [&](int q) -> float {
-            const float *w = sV + q * FV + vi;
-            return cx1 * (w[0] * mxm(gx) - w[SZ] * mxm(gx + 1)) - cx2 * (w[-SZ] * mxm(gx - 1) - w[2 * SZ] * mxm(gx + 2));
-        };
-        auto dzmT = [&](int q) -> float {
-            const float *w = sV + q * FV + vi;
-            return cz1 * (w[0] * mzm(gz) - w[1] * mzm(gz + 1)) - cz2 * (w[-1] * mzm(gz - 1) - w[2] * mzm(gz + 2));
-        };
-        const long long g = soff + (long long)gx * pitch + gz;
-        if (MODE == FWI_SH) {
-            a.sig_out[0][g] = sSig[si] + dxmT(0);
-            a.sig_out[1][g] = sSig[FS + si] + dzmT(0);
-        } else {
-            a.sig_out[0][g] = sSig[si] + dxmT(0);
-            a.sig_out[1][g] = sSig[FS + si] + dzmT(1);
-            a.sig_out[2][g] = sSig[2 * FS + si] + (dzmT(0) + dxmT(1));
-        }
-    }
-}
-
-// This step's gradient terms, all shots of the batch summed per cell in shot
-// order into FP64 accumulators ([nx][pitch]).  sig_adj: sig~ before the
-// transposed step (adjoint of sig(it+1)); vel_adj: v~ after it (= B a);
-// vf: forward v(it+1); dsf: forward divergence of step it.
-struct AdjPtrs {
-    const float *sig_adj[3], *vel_adj[2], *vf[2], *dsf[2];
-};
-
-template <int MODE>
-__global__ void grad_kernel(const AdjPtrs p, double *k_lam, double *k_mu, double *k_buo, int nx, int nz, int pitch,
-                            int nshots, float cx1, float cx2, float cz1, float cz2, double dt) {
-    const float *const *sig_adj = p.sig_adj;
-    const float *const *vel_adj = p.vel_adj;
-    const float *const *vf = p.vf;
-    const float *const *dsf = p.dsf;
-    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
-    if (j >= nz) return;
-    const bool okx = i >= 1 && i < nx - 2, okz = j >= 1 && j < nz - 2;
-    const long long o = (long long)i * pitch + j, field = (long long)nx * pitch;
-    double al = 0.0, am = 0.0, ab = 0.0;
-    for (int s = 0; s < nshots; s++) {
-        const long long g = s * field + o;
-        auto dxp = [&](const float *v) -> float {
-            return okx ? cx1 * (v[g + pitch] - v[g]) - cx2 * (v[g + 2 * pitch] - v[g - pitch]) : 0.f;
-        };
-        auto dzp = [&](const float *v) -> float {
-            return okz ? cz1 * (v[g + 1] - v[g]) - cz2 * (v[g + 2] - v[g - 1]) : 0.f;
-        };
-        if (MODE == FWI_SH) {
-            am += ((double)sig_adj[0][g] * dxp(vf[0]) + (double)sig_adj[1][g] * dzp(vf[0])) * dt;
-            ab += (double)vel_adj[0][g] * dsf[0][g];
-        } else {
-            const double exx = dxp(vf[0]), exz = dzp(vf[0]), ezx = dxp(vf[1]), ezz = dzp(vf[1]);
-            const double sxx = sig_adj[0][g], szz = sig_adj[1][g], sxz = sig_adj[2][g];
-            al += (sxx + szz) * (exx + ezz) * dt;
-            am += (2.0 * (sxx * exx + szz * ezz) + sxz * (exz + ezx)) * dt;
-            ab += (double)vel_adj[0][g] * dsf[0][g] + (double)vel_adj[1][g] * dsf[1][g];
-        }
-    }
-    if (k_lam && MODE != FWI_SH) k_lam[o] += al;
-    if (k_mu) k_mu[o] += am;
-    if (k_buo) k_buo[o] += ab;
-}
-
-// One transposed step (forward step `it`, adjoint state it+1 -> it) and its
-// gradient terms.
-int launch_adjoint_step(const fwi_batch *b, int it, cudaStream_t st) {
-    AdjArgs a;
-    a.nx = b->nx;
-    a.nz = b->nz;
-    a.pitch = b->pitch;
-    a.nt = b->nt;
-    a.it = it;
-    a.divnz = make_fastdiv(b->nz);
-    a.cx1 = (float)(9.0 / (8.0 * (double)b->dx));
-    a.cx2 = (float)(1.0 / (24.0 * (double)b->dx));
-    a.cz1 = (float)(9.0 / (8.0 * (double)b->dz));
-    a.cz2 = (float)(1.0 / (24.0 * (double)b->dz));
-    a.dt = (float)b->dt;
-    const int cur = b->cur, nxt = 1 - b->cur;
-    const int ns = b->mode == FWI_SH ? 2 : 3, nv = b->mode == FWI_SH ? 1 : 2;
-    for (int f = 0; f < 3; f++) {
-        a.sig_in[f] = f < ns ? b->sig[cur][f] : nullptr;
-        a.sig_out[f] = f < ns ? b->sig[nxt][f] : nullptr;
-    }
-    for (int q = 0; q < 2; q++) {
-        a.vel_in[q] = q < nv ? b->vel[cur][q] : nullptr;
-        a.vel_out[q] = q < nv ? b->vel[nxt][q] : nullptr;
-        a.disp[q] = q < nv ? b->disp[q] : nullptr;
-    }
-    a.buo = b->buo;
-    a.bound = b->bound;
-    a.lam = b->lam;
-    a.mu = b->mu;
-    a.inj_ptr = b->inj_ptr;
-    a.inj_cell = b->inj_cell;
-    a.inj_row = b->inj_row;
-    if (b->mode == FWI_SH) {
-        a.g[0] = b->stf[1];
-        a.g[1] = nullptr;
-    } else {
-        a.g[0] = b->stf[0];
-        a.g[1] = b->stf[2];
-    }
-    constexpr int TX = 32, TZ = 32;
-    dim3 grid((b->nz + TZ - 1) / TZ, (b->nx + TX - 1) / TX, b->nshots);
-    if (b->mode == FWI_SH) {
-        using T = AdjTile<FWI_SH, TX, TZ>;
-        static bool set = false;
-        if (!set) {
-            cudaError_t e = cudaFuncSetAttribute(adjoint_kernel<FWI_SH, TX, TZ>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::bytes);
-            if (e != cudaSuccess) return set_error(FWI_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
-            set = true;
-        }
-        adjoint_kernel<FWI_SH, TX, TZ><<<grid, kThreads, T::bytes, st>>>(a);
-    } else {
-        using T = AdjTile<FWI_PSV, TX, TZ>;
-        static bool set = false;
-        if (!set) {
-            cudaError_t e = cudaFuncSetAttribute(adjoint_kernel<FWI_PSV, TX, TZ>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::bytes);
-            if (e != cudaSuccess) return set_error(FWI_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
-            set = true;
-        }
-        adjoint_kernel<FWI_PSV, TX, TZ><<<grid, kThreads, T::bytes, st>>>(a);
-    }
-    int rc = check_launch("adjoint_kernel");
-    if (rc) return rc;
-    // gradient terms of this step
-    const long long field = (long long)b->nshots * b->nx * b->pitch;
-    const int slot = it - b->seg0;
-    const float *sa[3] = {a.sig_in[0], a.sig_in[1], a.sig_in[2]};
-    const float *va[2] = {a.vel_out[0], a.vel_out[1]};
-    const int cx = b->mode == FWI_SH ? 1 : 0, czs = b->mode == FWI_SH ? 1 : 2;
-    const float *vf[2] = {b->seg_v[cx] + slot * field, nv > 1 ? b->seg_v[czs] + slot * field : nullptr};
-    const float *df[2] = {b->seg_ds[cx] + slot * field, nv > 1 ? b->seg_ds[czs] + slot * field : nullptr};
-    dim3 g2((b->nz + 127) / 128, b->nx);
-    AdjPtrs ptrs;
-    for (int f = 0; f < 3; f++) ptrs.sig_adj[f] = sa[f];
-    for (int q = 0; q < 2; q++) {
-        ptrs.vel_adj[q] = va[q];
-        ptrs.vf[q] = vf[q];
-        ptrs.dsf[q] = df[q];
-    }
-    if (b->mode == FWI_SH)
-        grad_kernel<FWI_SH><<<g2, 128, 0, st>>>(ptrs, nullptr, b->k_mu, b->k_rho, b->nx, b->nz, b->pitch, b->nshots,
-                                               a.cx1, a.cx2, a.cz1, a.cz2, b->dt);
-    else
-        grad_kernel<FWI_PSV><<<g2, 128, 0, st>>>(ptrs, b->k_lam, b->k_mu, b->k_rho, b->nx, b->nz, b->pitch,
-                                                b->nshots, a.cx1, a.cx2, a.cz1, a.cz2, b->dt);
-    return check_launch("grad_kernel");
-}
-
 // ------------------------------------------------------------- launching
 
 struct TileShape {
@@ -1357,6 +1057,525 @@ int multi_run(fwi_batch *const *bs, int n, void *ws, int it0, int nsteps, cudaSt
     delete[] order;
     delete[] prefix;
     return rc;
+}
+
+// ------------------------------------------------ exact discrete adjoint
+//
+// The forward step above is linear in the state.  For SH / P-SV it reads
+//   d  = D- sig + f            (stress divergence plus sources)
+//   v' = B (v + b d)           (b = dt/rho, B = sponge)
+//   u' = u + dt v'
+//   sig' = sig + dt S(D+ v')   (S: lam/mu stress-strain law)
+// Its exact transpose, run backwards in time on the adjoint state, is
+//   a    = v~ + dt u~ + (D+)^T (dt S^T sig~)
+//   v~'  = B a
+//   sig~' = sig~ + (D-)^T (b v~')
+// with (D+)^T and (D-)^T the transposes of the reference's masked stencils
+// (solver.py:22-51), boundary masks included, so the adjoint is exact to
+// rounding.  The displacement feeds nothing but the receivers, so its
+// adjoint u~ is zero away from them and equals, at a receiver, the sum of
+// dL/d(trace) over the steps still to come: the caller passes those suffix
+// sums (fwi_trace_suffix_sum) as the injection values and u~ never exists
+// as a field.  The same launch adds this step's gradient terms
+//   dL/dlam = sum dt (sxx~+szz~)(exx+ezz),
+//   dL/dmu  = sum dt (2 sxx~ exx + 2 szz~ ezz + sxz~ (exz+ezx))  [SH: dt (sxy~ exy + szy~ ezy)]
+//   dL/db   = sum v~' . d
+// (sig~ before the step; e = D+ of the forward v', v' and d stored per step
+// by a recomputed forward segment).
+//
+// Mapping.  A cluster of C <= 8 CTAs owns one 32 x 32 tile; CTA r of the
+// cluster processes shots r, r+C, ... in turn, keeping the model tile
+// (stiffness with halo, dt/rho, sponge) in shared memory across its shots
+// and its gradient terms in registers.  Per shot it stages sig~, v~ and the
+// forward v' with TMA, forms t = dt S^T sig~ in place, computes v~' on the
+// interior (lane = z, x taps in a register window, as step_kernel_rw) plus
+// the halo, then sig~' and the gradient terms of the interior.  At the end
+// the cluster sums its CTAs' terms through distributed shared memory in
+// rank order and adds them once into the FP64 gradient arrays: one
+// read-modify-write per cell and step for all shots, deterministic, no
+// atomics.
+
+struct AdjArgs {
+    int nx, nz, pitch, nt, it, nshots;
+    FastDiv divnz;
+    float cx1, cx2, cz1, cz2, dt;
+    float *sig_out[3];
+    float *vel_out[2];
+    const float *dsf[2];   // forward divergence of step it, per component
+    double *k[3];          // SH: dL/dmu, dL/dbuo | P-SV: dL/dlam, dL/dmu, dL/dbuo ([nx][pitch], NULL skips)
+    const int *inj_ptr, *inj_cell, *inj_row;
+    const float *g[2];     // u~ at the receivers per step (forward time order)
+};
+
+struct AdjMaps {
+    CUtensorMap sig[3];  // sig~, stress region box
+    CUtensorMap vel[2];  // v~, velocity region box
+    CUtensorMap vf[2];   // forward v(it+1), velocity region box
+    CUtensorMap lm[2];   // SH: mu | P-SV: lam, mu; stress region box
+    CUtensorMap vp[2];   // dt/rho, sponge; velocity region box
+};
+
+template <int MODE>
+struct AdjTile {
+    using F = Fields<MODE>;
+    static constexpr int TX = 32, TZ = 32;
+    static constexpr int SX = TX + 6, SZ = TZ + 8, VX = TX + 3, RVZ = TZ + 3;
+    static constexpr int FS = (SX * SZ + 31) / 32 * 32, FV = (VX * SZ + 31) / 32 * 32;
+    static constexpr int NL = MODE == FWI_SH ? 1 : 2;  // stiffness fields
+    static constexpr int NK = MODE == FWI_SH ? 2 : 3;  // gradient fields
+    // per-shot region (sig~, v~, forward v'), then the model tile, the
+    // injection list and two mbarriers (model, shot)
+    static constexpr int V_OFF = F::NS * FS, VF_OFF = V_OFF + F::NV * FV;
+    static constexpr int L_OFF = VF_OFF + F::NV * FV, P_OFF = L_OFF + NL * FS;
+    static constexpr int LIST_OFF = P_OFF + 2 * FV;
+    static constexpr int LIST = kThreads * (1 + F::NINJ) + 8;
+    static constexpr int BAR_OFF = (LIST_OFF + LIST + 1) / 2 * 2;
+    static constexpr size_t bytes = sizeof(float) * (size_t)(BAR_OFF + 4);
+    static constexpr uint32_t shot_bytes = 4u * (F::NS * SX * SZ + 2 * F::NV * VX * SZ);
+    static constexpr uint32_t model_bytes = 4u * (NL * SX * SZ + 2 * VX * SZ);
+    static_assert(NK * TX * TZ <= L_OFF, "gradient terms overlay the per-shot region");
+    static_assert(shot_bytes < (1u << 20) && model_bytes < (1u << 20), "mbarrier transaction count limit");
+};
+
+// Injection of u~ for one shot: entries whose cell lies in the computed
+// velocity region add dt * u~ to the staged v~, summed per cell in entry
+// order.  adj_collect compacts up to kThreads entries [base, p1) into the
+// list (block-wide; the count it returns is block-uniform) and may run
+// while the staging copies are in flight; adj_apply adds them once v~ has
+// landed and the list is visible to thread 0.
+template <int MODE>
+__device__ __forceinline__ int adj_collect(const AdjArgs &a, int base, int p1, int x0, int z0, int *sLoc,
+                                           float *sVal, int *sWarp) {
+    using T = AdjTile<MODE>;
+    constexpr int NINJ = Fields<MODE>::NINJ;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int e = base + tid;
+    int loc = -1;
+    float val[NINJ];
+    if (e < p1) {
+        const int k = a.inj_cell[e];
+        const int gx = fdiv(k, a.divnz), gz = k - gx * a.nz;
+        const int rx = gx - (x0 - 1), rz = gz - (z0 - 1);
+        if (rx >= 0 && rx < T::VX && rz >= 0 && rz < T::RVZ) {
+            loc = rx * T::SZ + rz + 3;
+            const long long src = (long long)a.inj_row[e] * a.nt + a.it;
+#pragma unroll
+            for (int c = 0; c < NINJ; c++) val[c] = a.g[c][src];
+        }
+    }
+    const unsigned ball = __ballot_sync(0xffffffffu, loc >= 0);
+    if (lane == 0) sWarp[warp] = __popc(ball);
+    __syncthreads();
+    int n = 0, pos = __popc(ball & ((1u << lane) - 1u));
+    for (int w = 0; w < kThreads / 32; w++) {
+        if (w < warp) pos += sWarp[w];
+        n += sWarp[w];
+    }
+    if (loc >= 0) {
+        sLoc[pos] = loc;
+#pragma unroll
+        for (int c = 0; c < NINJ; c++) sVal[c * kThreads + pos] = val[c];
+    }
+    return n;
+}
+
+template <int MODE>
+__device__ __forceinline__ void adj_apply(float *sV, int n, const int *sLoc, const float *sVal, float dt) {
+    if (threadIdx.x != 0) return;
+    for (int q = 0; q < n; q++) {
+#pragma unroll
+        for (int c = 0; c < Fields<MODE>::NINJ; c++)
+            sV[c * AdjTile<MODE>::FV + sLoc[q]] += dt * sVal[c * kThreads + q];
+    }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : 3)
+    adjoint_kernel(const __grid_constant__ AdjArgs a, const __grid_constant__ AdjMaps m) {
+    using T = AdjTile<MODE>;
+    using F = Fields<MODE>;
+    constexpr int TX = T::TX, TZ = T::TZ, SX = T::SX, SZ = T::SZ, RVZ = T::RVZ, FS = T::FS, FV = T::FV;
+    constexpr int NS = F::NS, NV = F::NV, NL = T::NL, NK = T::NK, RPW = TX / (kThreads / 32);
+    extern __shared__ __align__(128) float smem[];
+    float *sS = smem, *sV = smem + T::V_OFF, *sF = smem + T::VF_OFF, *sL = smem + T::L_OFF, *sP = smem + T::P_OFF;
+    int *sLoc = reinterpret_cast<int *>(smem + T::LIST_OFF);
+    float *sVal = reinterpret_cast<float *>(sLoc + kThreads);
+    int *sWarp = reinterpret_cast<int *>(sVal + F::NINJ * kThreads);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + T::BAR_OFF);
+    cg::cluster_group cluster = cg::this_cluster();
+    const int crank = (int)cluster.block_rank(), csize = (int)cluster.num_blocks();
+
+    const int tid = threadIdx.x, lane = tid & 31, ix0 = (tid >> 5) * RPW;
+    const int z0 = blockIdx.x * TZ, x0 = blockIdx.y * TX;
+    const int nx = a.nx, nz = a.nz, pitch = a.pitch;
+    const int gz = z0 + lane, col = lane + 4;
+    const bool zin = gz < nz;
+    const float dt = a.dt, cx1 = a.cx1, cx2 = a.cx2, cz1 = a.cz1, cz2 = a.cz2;
+    // z masks of this lane: (D+)^T taps gz-2..gz+1, (D-)^T taps gz-1..gz+2
+    float pz[4], mz[4];
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+        const int kp = gz - 2 + d, km = gz - 1 + d;
+        pz[d] = (kp >= 1 && kp < nz - 2) ? 1.f : 0.f;
+        mz[d] = (km >= 2 && km < nz - 2) ? 1.f : 0.f;
+    }
+    const bool okz = gz >= 1 && gz < nz - 2;
+
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+        mbar_expect_tx(&bar[0], T::model_bytes);
+#pragma unroll
+        for (int f = 0; f < NL; f++) tma_load_2d(sL + f * FS, &m.lm[f], z0 - 4, x0 - 3, &bar[0]);
+#pragma unroll
+        for (int p = 0; p < 2; p++) tma_load_2d(sP + p * FV, &m.vp[p], z0 - 4, x0 - 1, &bar[0]);
+    }
+
+    float gk[NK][RPW];
+#pragma unroll
+    for (int k = 0; k < NK; k++)
+#pragma unroll
+        for (int q = 0; q < RPW; q++) gk[k][q] = 0.f;
+
+    int iter = 0;
+    bool failed = false;
+    for (int shot = crank; shot < a.nshots; shot += csize, iter++) {
+        const long long soff = (long long)shot * nx * pitch;
+        if (tid == 0) {
+            // the previous shot's generic-proxy accesses of this memory are ordered before the copies
+            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+            mbar_expect_tx(&bar[1], T::shot_bytes);
+#pragma unroll
+            for (int f = 0; f < NS; f++) tma_load_3d(sS + f * FS, &m.sig[f], z0 - 4, x0 - 3, shot, &bar[1]);
+#pragma unroll
+            for (int q = 0; q < NV; q++) tma_load_3d(sV + q * FV, &m.vel[q], z0 - 4, x0 - 1, shot, &bar[1]);
+#pragma unroll
+            for (int q = 0; q < NV; q++) tma_load_3d(sF + q * FV, &m.vf[q], z0 - 4, x0 - 1, shot, &bar[1]);
+        }
+        // forward divergence of the interior cells (read once: straight from HBM)
+        float dsv[NV][RPW];
+#pragma unroll
+        for (int q = 0; q < RPW; q++) {
+            const int gx = x0 + ix0 + q;
+            const bool in = zin && gx < nx;
+#pragma unroll
+            for (int c = 0; c < NV; c++) dsv[c][q] = in ? a.dsf[c][soff + (long long)gx * pitch + gz] : 0.f;
+        }
+        const int p0 = a.inj_ptr ? a.inj_ptr[shot] : 0, p1 = a.inj_ptr ? a.inj_ptr[shot + 1] : 0;
+        const bool single = p1 - p0 <= kThreads;
+        int n_in = 0;
+        if (single && p1 > p0) n_in = adj_collect<MODE>(a, p0, p1, x0, z0, sLoc, sVal, sWarp);
+        bool ok = mbar_wait(&bar[1], iter & 1);
+        if (iter == 0) ok = mbar_wait(&bar[0], 0) && ok;
+        if (__syncthreads_or(!ok)) {  // block-uniform decision
+            if (tid == 0) atomicExch(&g_device_status, 1);
+            mbar_wait(&bar[1], iter & 1);  // one more bounded chance for copies in flight
+            if (iter == 0) mbar_wait(&bar[0], 0);
+            failed = true;
+            break;
+        }
+        if (single) {
+            adj_apply<MODE>(sV, n_in, sLoc, sVal, dt);
+        } else {
+            for (int base = p0; base < p1; base += kThreads) {
+                __syncthreads();
+                const int n = adj_collect<MODE>(a, base, p1, x0, z0, sLoc, sVal, sWarp);
+                __syncthreads();
+                adj_apply<MODE>(sV, n, sLoc, sVal, dt);
+            }
+        }
+        // sig~ of the interior cells into registers (t overwrites it)
+        float sg[NS][RPW];
+#pragma unroll
+        for (int f = 0; f < NS; f++)
+#pragma unroll
+            for (int q = 0; q < RPW; q++) sg[f][q] = sS[f * FS + (ix0 + q + 3) * SZ + col];
+        __syncthreads();
+        // t = dt S^T sig~ in place, stress region rows, columns z0-3 .. z0+TZ+2
+        for (int c = tid; c < SX * (SZ - 2); c += kThreads) {
+            const int r = c / (SZ - 2), i = r * SZ + (c - r * (SZ - 2)) + 1;
+            if (MODE == FWI_SH) {
+                const float mu = sL[i];
+                sS[i] = dt * (mu * sS[i]);
+                sS[FS + i] = dt * (mu * sS[FS + i]);
+            } else {
+                const float l = sL[i], mu = sL[FS + i], l2m = l + 2.f * mu;
+                const float sxx = sS[i], szz = sS[FS + i], sxz = sS[2 * FS + i];
+                sS[i] = dt * (l2m * sxx + l * szz);
+                sS[FS + i] = dt * (l * sxx + l2m * szz);
+                sS[2 * FS + i] = dt * (mu * sxz);
+            }
+        }
+        __syncthreads();
+
+        // ---- v~' on the warp's interior rows; t rows x-2 .. x+1 of the
+        // x-differentiated fields in a register window, pre-masked
+        // (window index r <-> stress row ix0+1+r <-> grid row x0+ix0-2+r)
+        {
+            float w[NS][RPW + 3];
+#pragma unroll
+            for (int f = 0; f < NS; f++)
+                if (takes_dxm(MODE, f)) {
+#pragma unroll
+                    for (int r = 0; r < RPW + 3; r++) {
+                        const int gr = x0 + ix0 - 2 + r;
+                        w[f][r] = (gr >= 1 && gr < nx - 2) ? sS[f * FS + (ix0 + 1 + r) * SZ + col] : 0.f;
+                    }
+                }
+#pragma unroll
+            for (int q = 0; q < RPW; q++) {
+                const int ix = ix0 + q, gx = x0 + ix;
+                const int vi = (ix + 1) * SZ + col;
+                if (!(zin && gx < nx)) {
+#pragma unroll
+                    for (int c = 0; c < NV; c++) sV[c * FV + vi] = 0.f;
+                    continue;
+                }
+                const float *trow = sS + (ix + 3) * SZ + col;
+                auto dxpT = [&](int f) -> float {
+                    return cx1 * (w[f][q + 1] - w[f][q + 2]) - cx2 * (w[f][q] - w[f][q + 3]);
+                };
+                auto dzpT = [&](int f) -> float {
+                    const float *t = trow + f * FS;
+                    return cz1 * (t[-1] * pz[1] - t[0] * pz[2]) - cz2 * (t[-2] * pz[0] - t[1] * pz[3]);
+                };
+                float acc[2];
+                if (MODE == FWI_SH) {
+                    acc[0] = dxpT(0) + dzpT(1);
+                } else {
+                    acc[0] = dxpT(0) + dzpT(2);
+                    acc[1] = dxpT(2) + dzpT(1);
+                }
+                const float buo = sP[vi], bnd = sP[FV + vi];
+                const long long g = soff + (long long)gx * pitch + gz;
+                float gb = 0.f;
+#pragma unroll
+                for (int c = 0; c < NV; c++) {
+                    const float vn = bnd * (sV[c * FV + vi] + acc[c]);
+                    sV[c * FV + vi] = buo * vn;
+                    a.vel_out[c][g] = vn;
+                    gb += vn * dsv[c][q];
+                }
+                gk[NK - 1][q] += gb;
+            }
+        }
+        // ---- v~' on the halo rows x0-1, x0+TX, x0+TX+1 and columns z0-1,
+        // z0+TZ, z0+TZ+1 (redundant with the neighbour tiles; masks per tap)
+        {
+            constexpr int HROW = 3 * RVZ, HC = HROW + 3 * TX;
+            auto mxp = [&](int k) -> float { return (k >= 1 && k < nx - 2) ? 1.f : 0.f; };
+            auto mzp = [&](int k) -> float { return (k >= 1 && k < nz - 2) ? 1.f : 0.f; };
+            for (int c = tid; c < HC; c += kThreads) {
+                int rx, rz;
+                if (c < HROW) {
+                    const int r3 = c / RVZ;
+                    rx = r3 == 0 ? 0 : TX + r3;
+                    rz = c - r3 * RVZ;
+                } else {
+                    const int c2 = c - HROW, k3 = c2 % 3;
+                    rx = 1 + c2 / 3;
+                    rz = k3 == 0 ? 0 : TZ + k3;
+                }
+                const int hx = x0 - 1 + rx, hz = z0 - 1 + rz;
+                const int vi = rx * SZ + rz + 3, si = (rx + 2) * SZ + rz + 3;
+                if (hx < 0 || hx >= nx || hz < 0 || hz >= nz) {
+#pragma unroll
+                    for (int q = 0; q < NV; q++) sV[q * FV + vi] = 0.f;
+                    continue;
+                }
+                auto dxpT = [&](int f) -> float {
+                    const float *t = sS + f * FS + si;
+                    return cx1 * (t[-SZ] * mxp(hx - 1) - t[0] * mxp(hx)) -
+                           cx2 * (t[-2 * SZ] * mxp(hx - 2) - t[SZ] * mxp(hx + 1));
+                };
+                auto dzpT = [&](int f) -> float {
+                    const float *t = sS + f * FS + si;
+                    return cz1 * (t[-1] * mzp(hz - 1) - t[0] * mzp(hz)) - cz2 * (t[-2] * mzp(hz - 2) - t[1] * mzp(hz + 1));
+                };
+                float acc[2];
+                if (MODE == FWI_SH) {
+                    acc[0] = dxpT(0) + dzpT(1);
+                } else {
+                    acc[0] = dxpT(0) + dzpT(2);
+                    acc[1] = dxpT(2) + dzpT(1);
+                }
+                const float buo = sP[vi], bnd = sP[FV + vi];
+#pragma unroll
+                for (int q = 0; q < NV; q++) sV[q * FV + vi] = buo * (bnd * (sV[q * FV + vi] + acc[q]));
+            }
+        }
+        __syncthreads();
+
+        // ---- sig~' and the stiffness gradient terms on the interior; b v~'
+        // (pre-masked) and the forward v' rows x-1 .. x+2 in register windows
+        // (window index r <-> velocity row ix0+r <-> grid row x0+ix0-1+r)
+        {
+            float w[NV][RPW + 3], f[NV][RPW + 3];
+#pragma unroll
+            for (int c = 0; c < NV; c++) {
+#pragma unroll
+                for (int r = 0; r < RPW + 3; r++) {
+                    const int gr = x0 + ix0 - 1 + r;
+                    w[c][r] = (gr >= 2 && gr < nx - 2) ? sV[c * FV + (ix0 + r) * SZ + col] : 0.f;
+                    f[c][r] = sF[c * FV + (ix0 + r) * SZ + col];
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < RPW; q++) {
+                const int ix = ix0 + q, gx = x0 + ix;
+                if (!(zin && gx < nx)) continue;
+                const bool okx = gx >= 1 && gx < nx - 2;
+                const float *vrow = sV + (ix + 1) * SZ + col, *frow = sF + (ix + 1) * SZ + col;
+                auto dxmT = [&](int c) -> float {
+                    return cx1 * (w[c][q + 1] - w[c][q + 2]) - cx2 * (w[c][q] - w[c][q + 3]);
+                };
+                auto dzmT = [&](int c) -> float {
+                    const float *v = vrow + c * FV;
+                    return cz1 * (v[0] * mz[1] - v[1] * mz[2]) - cz2 * (v[-1] * mz[0] - v[2] * mz[3]);
+                };
+                auto dxp = [&](int c) -> float {
+                    return okx ? cx1 * (f[c][q + 2] - f[c][q + 1]) - cx2 * (f[c][q + 3] - f[c][q]) : 0.f;
+                };
+                auto dzp = [&](int c) -> float {
+                    const float *v = frow + c * FV;
+                    return okz ? cz1 * (v[1] - f[c][q + 1]) - cz2 * (v[2] - v[-1]) : 0.f;
+                };
+                const long long g = soff + (long long)gx * pitch + gz;
+                if (MODE == FWI_SH) {
+                    a.sig_out[0][g] = sg[0][q] + dxmT(0);
+                    a.sig_out[1][g] = sg[1][q] + dzmT(0);
+                    gk[0][q] += dt * (sg[0][q] * dxp(0) + sg[1][q] * dzp(0));
+                } else {
+                    a.sig_out[0][g] = sg[0][q] + dxmT(0);
+                    a.sig_out[1][g] = sg[1][q] + dzmT(1);
+                    a.sig_out[2][g] = sg[2][q] + (dzmT(0) + dxmT(1));
+                    const float exx = dxp(0), exz = dzp(0), ezx = dxp(1), ezz = dzp(1);
+                    const float sxx = sg[0][q], szz = sg[1][q], sxz = sg[2][q];
+                    gk[0][q] += dt * ((sxx + szz) * (exx + ezz));
+                    gk[1][q] += dt * (2.f * (sxx * exx + szz * ezz) + sxz * (exz + ezx));
+                }
+            }
+        }
+        __syncthreads();  // shared memory is refilled for the next shot
+    }
+    if (iter == 0 && !failed) mbar_wait(&bar[0], 0);  // no shot: let the model copies land
+
+    // ---- cluster sum of the gradient terms, in rank order, into FP64
+    float *part = smem;
+#pragma unroll
+    for (int k = 0; k < NK; k++)
+#pragma unroll
+        for (int q = 0; q < RPW; q++) part[k * TX * TZ + (ix0 + q) * TZ + lane] = gk[k][q];
+    cluster.sync();
+    const int chunk = (TX * TZ + csize - 1) / csize, c0 = crank * chunk;
+    for (int e = tid; e < NK * chunk; e += kThreads) {
+        const int k = e / chunk, c = c0 + (e - k * chunk);
+        if (c >= TX * TZ || !a.k[k]) continue;
+        const int gx = x0 + c / TZ, gzc = z0 + c % TZ;
+        if (gx >= nx || gzc >= nz) continue;
+        double s = 0.0;
+        for (int j = 0; j < csize; j++) s += (double)cluster.map_shared_rank(part, j)[k * TX * TZ + c];
+        a.k[k][(long long)gx * pitch + gzc] += s;
+    }
+    cluster.sync();  // keep this CTA's shared memory alive until every rank has read it
+}
+
+// Tensor maps of one transposed step.
+template <int MODE>
+static int adjoint_maps(const fwi_batch *b, const float *const *vf, AdjMaps &m) {
+    using T = AdjTile<MODE>;
+    using F = Fields<MODE>;
+    const int cur = b->cur, nx = b->nx, pitch = b->pitch, ns = b->nshots;
+    int rc = 0;
+    for (int f = 0; f < F::NS && !rc; f++) rc = encode_map(&m.sig[f], b->sig[cur][f], 3, pitch, nx, ns, T::SZ, T::SX);
+    for (int q = 0; q < F::NV && !rc; q++) rc = encode_map(&m.vel[q], b->vel[cur][q], 3, pitch, nx, ns, T::SZ, T::VX);
+    for (int q = 0; q < F::NV && !rc; q++) rc = encode_map(&m.vf[q], vf[q], 3, pitch, nx, ns, T::SZ, T::VX);
+    const float *lm[2] = {MODE == FWI_SH ? b->mu : b->lam, b->mu};
+    for (int f = 0; f < T::NL && !rc; f++) rc = encode_map(&m.lm[f], lm[f], 2, pitch, nx, 1, T::SZ, T::SX);
+    const float *vp[2] = {b->buo, b->bound};
+    for (int p = 0; p < 2 && !rc; p++) rc = encode_map(&m.vp[p], vp[p], 2, pitch, nx, 1, T::SZ, T::VX);
+    return rc;
+}
+
+// Shots per cluster of the transposed step (portable cluster size limit 8).
+static int adjoint_cluster(int nshots) { return nshots < 8 ? nshots : 8; }
+
+template <int MODE>
+static int launch_adjoint(const fwi_batch *b, const AdjArgs &a, const float *const *vf, cudaStream_t st) {
+    using T = AdjTile<MODE>;
+    static bool set = false;
+    if (!set) {
+        cudaError_t e = cudaFuncSetAttribute(adjoint_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)T::bytes);
+        if (e != cudaSuccess) return set_error(FWI_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+        set = true;
+    }
+    AdjMaps m;
+    int rc = adjoint_maps<MODE>(b, vf, m);
+    if (rc) return rc;
+    const int C = adjoint_cluster(b->nshots);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((b->nz + T::TZ - 1) / T::TZ, (b->nx + T::TX - 1) / T::TX, C);
+    cfg.blockDim = dim3(kThreads, 1, 1);
+    cfg.dynamicSmemBytes = T::bytes;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 1;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = C;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, adjoint_kernel<MODE>, a, m);
+    if (e != cudaSuccess) return set_error(FWI_ECUDA, "adjoint_kernel launch: %s", cudaGetErrorString(e));
+    return check_launch("adjoint_kernel");
+}
+
+// One transposed step (forward step `it`, adjoint state it+1 -> it) with
+// its gradient terms.
+int launch_adjoint_step(const fwi_batch *b, int it, cudaStream_t st) {
+    AdjArgs a;
+    a.nx = b->nx;
+    a.nz = b->nz;
+    a.pitch = b->pitch;
+    a.nt = b->nt;
+    a.it = it;
+    a.nshots = b->nshots;
+    a.divnz = make_fastdiv(b->nz);
+    a.cx1 = (float)(9.0 / (8.0 * (double)b->dx));
+    a.cx2 = (float)(1.0 / (24.0 * (double)b->dx));
+    a.cz1 = (float)(9.0 / (8.0 * (double)b->dz));
+    a.cz2 = (float)(1.0 / (24.0 * (double)b->dz));
+    a.dt = (float)b->dt;
+    const bool sh = b->mode == FWI_SH;
+    const int nxt = 1 - b->cur, ns = sh ? 2 : 3, nv = sh ? 1 : 2;
+    for (int f = 0; f < 3; f++) a.sig_out[f] = f < ns ? b->sig[nxt][f] : nullptr;
+    for (int q = 0; q < 2; q++) a.vel_out[q] = q < nv ? b->vel[nxt][q] : nullptr;
+    const long long field = (long long)b->nshots * b->nx * b->pitch;
+    const long long slot = it - b->seg0;
+    const int cx = sh ? 1 : 0;
+    const float *vf[2] = {b->seg_v[cx] + slot * field, sh ? nullptr : b->seg_v[2] + slot * field};
+    a.dsf[0] = b->seg_ds[cx] + slot * field;
+    a.dsf[1] = sh ? nullptr : b->seg_ds[2] + slot * field;
+    if (sh) {
+        a.k[0] = b->k_mu;
+        a.k[1] = b->k_rho;
+        a.k[2] = nullptr;
+    } else {
+        a.k[0] = b->k_lam;
+        a.k[1] = b->k_mu;
+        a.k[2] = b->k_rho;
+    }
+    a.inj_ptr = b->inj_ptr;
+    a.inj_cell = b->inj_cell;
+    a.inj_row = b->inj_row;
+    a.g[0] = sh ? b->stf[1] : b->stf[0];
+    a.g[1] = sh ? nullptr : b->stf[2];
+    return sh ? launch_adjoint<FWI_SH>(b, a, vf, st) : launch_adjoint<FWI_PSV>(b, a, vf, st);
 }
 
 }  // namespace fwi

@@ -327,6 +327,18 @@ def misfit_tracegrad(data: torch.Tensor, syn: torch.Tensor, grad: torch.Tensor, 
     return out
 
 
+def trace_suffix_sum(g: torch.Tensor, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    """Suffix sums along the last (time) axis, FP64-accumulated
+    (fwi_trace_suffix_sum): the adjoint displacement at the receivers that
+    fwi_run_transposed injects.  out may be g itself."""
+    if out is None:
+        out = torch.empty_like(g)
+    nt = g.shape[-1]
+    check(_lib.load().fwi_trace_suffix_sum(ptr(g), ptr(out), g.numel() // max(nt, 1), nt, stream_handle(stream)),
+          "fwi_trace_suffix_sum")
+    return out
+
+
 def smooth(k: torch.Tensor, grid: Grid, sigma: int, stream=None) -> torch.Tensor:
     """Gaussian smoothing of an FP64 [nx, pitch] kernel into float32 [npt]."""
     out = torch.empty(grid.npt, dtype=torch.float32, device=k.device)

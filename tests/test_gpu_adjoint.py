@@ -214,3 +214,58 @@ def test_plugin_psv_gradient_is_dt_times_exact(tmp_path):
     chi.backward()
     ref = 1e-3 * mu.grad.double().cpu().numpy()
     assert np.linalg.norm(kraw - ref) / np.linalg.norm(ref) < 1e-5
+
+
+def test_trace_suffix_sum():
+    from seispie_b200 import engine
+    rng = np.random.default_rng(8)
+    for ntr, nt in ((7, 1), (5, 256), (9, 1000), (3, 4097)):
+        g = rng.standard_normal((ntr, nt)).astype(np.float32)
+        want = np.flip(np.cumsum(np.flip(g.astype(np.float64), -1), -1), -1)
+        gt = torch.as_tensor(g).cuda()
+        out = engine.trace_suffix_sum(gt)
+        np.testing.assert_allclose(out.cpu().numpy(), want, rtol=1e-6, atol=1e-5)
+        engine.trace_suffix_sum(gt, gt)  # in place
+        assert torch.equal(gt, out)
+
+
+def _wide_case(mode, nshots=11, nrec=300, nx=70, nz=66, nt=200):
+    """Several tiles, more shots than a cluster, more receivers than a CTA
+    compacts at once, receivers on and next to tile edges."""
+    from seispie_b200.adjoint import AcquisitionSetup
+    from seispie_b200.engine import Grid
+    setup, p, src, rec, absorb, rng = _case(mode, seed=11, nx=nx, nz=nz, nt=nt)
+    h = setup.grid.dx
+    src = np.array([[h * (6 + 5 * s), h * (8 + (7 * s) % 50), 0, 14.0, 0.07 + 0.003 * s, 10.0 * s, 1e10]
+                    for s in range(nshots)])
+    xs = [30, 31, 32, 33, 34, 63, 64, 65, 2, 5, 47]
+    rec = np.array([[h * xs[r % len(xs)], h * (3 + (r * 7) % (nz - 6))] for r in range(nrec)])
+    setup = AcquisitionSetup(mode, Grid(nx, nz, h, h), setup.dt, nt, src, rec, absorb, segment=23)
+    return setup, p, src, rec, absorb
+
+
+@pytest.mark.parametrize("mode", ["sh", "psv"])
+def test_exact_gradient_many_shots_tiles_receivers(mode):
+    from seispie_b200.adjoint import AcquisitionSetup
+    setup, p, src, rec, absorb = _wide_case(mode)
+    data = _data(setup, p, src, absorb)
+    grad, _ = _gpu_grad(setup, p, data)
+    g = setup.grid
+    i, j = np.meshgrid(np.arange(g.nx), np.arange(g.nz), indexing="ij")
+    direction = {k: (0.5 + 0.5 * np.sin(0.17 * i + 0.11 * j + n)) * p[k] for n, k in enumerate(p)}
+    eps = 1e-5
+    pp = {k: p[k].astype(np.float64) + eps * direction[k] for k in p}
+    pm = {k: p[k].astype(np.float64) - eps * direction[k] for k in p}
+    fd = (_oracle_chi(setup, pp, src, absorb, data) - _oracle_chi(setup, pm, src, absorb, data)) / (2 * eps)
+    dd = sum(float((grad[k] * direction[k]).sum()) for k in p)
+    assert abs(dd - fd) < 1e-4 * abs(fd), (dd, fd)
+    # the batched gradient is the sum of the one-shot gradients
+    total = {k: np.zeros_like(v) for k, v in grad.items()}
+    for s in range(len(src)):
+        one = AcquisitionSetup(mode, g, setup.dt, setup.nt, src[s:s + 1], rec, absorb, segment=23)
+        gs, _ = _gpu_grad(one, p, data[:, s:s + 1])
+        for k in total:
+            total[k] += gs[k]
+    for k in grad:
+        scale = np.abs(grad[k]).max()
+        np.testing.assert_allclose(grad[k], total[k], rtol=0, atol=2e-5 * scale, err_msg=k)
