@@ -99,12 +99,14 @@ typedef struct fwi_batch {
     float *snap_u[3];
     float *snap_v[3];
     double *k_lam, *k_mu, *k_rho;
-    /* Exact discrete adjoint (fwi_run_transposed).  Forward runs with these
-     * set also store, for every step it with 0 <= it-seg0 < nseg, the new
-     * velocity v(it+1) into seg_v[c] and the stress divergence including the
-     * sources of step it into seg_ds[c], at slot it-seg0 of
-     * [nseg][nshots][nx][pitch] buffers (component slots as obs).  NULL skips. */
-    float *seg_v[3];
+    /* Exact discrete adjoint (fwi_run_transposed).  SH / P-SV forward runs
+     * with these set also store, for every step it with 0 <= it-seg0 < nseg,
+     * at slot it-seg0 of [nseg][nshots][nx][pitch] buffers: the strain of the
+     * new velocity v(it+1) (D+ of it, masked as the stress update uses it)
+     * into seg_e[k] -- SH: exy, ezy; P-SV: exx, ezz, exz+ezx -- and the stress
+     * divergence including the sources of step it into seg_ds[c] (component
+     * slots as obs).  NULL skips. */
+    float *seg_e[3];
     float *seg_ds[3];
     int seg0, nseg;
 } fwi_batch;
@@ -198,8 +200,8 @@ int fwi_multi_run(fwi_batch *const *batches, int n, void *workspace, int it0, in
  * fwi_run's injection, typically one per receiver and shot) and enters v~ as
  * dt * u~ at inj_cell[e].  Each step also accumulates, over every shot, into
  * the FP64 arrays: dL/dlam (k_lam, P-SV), dL/dmu (k_mu), dL/dbuo with buo =
- * dt/rho (k_rho); NULL skips an array.  Needs the forward v(it+1) and
- * divergence of step it in seg_v / seg_ds for every step of the range
+ * dt/rho (k_rho); NULL skips an array.  Needs the forward strain of v(it+1)
+ * and divergence of step it in seg_e / seg_ds for every step of the range
  * (written by a forward fwi_run over the same segment).  No counterpart in
  * the reference, whose adjoint (solver.py:290-329) is the continuous-adjoint
  * approximation fwi_run's adjoint = 1 reproduces. */

@@ -33,7 +33,7 @@ class FwiBatch(ctypes.Structure):
         ("nrec", ctypes.c_int), ("rec_cell", _vp), ("obs", _vp * 3),
         ("sae", ctypes.c_int), ("nsa", ctypes.c_int), ("snap_u", _vp * 3), ("snap_v", _vp * 3),
         ("k_lam", _vp), ("k_mu", _vp), ("k_rho", _vp),
-        ("seg_v", _vp * 3), ("seg_ds", _vp * 3), ("seg0", ctypes.c_int), ("nseg", ctypes.c_int),
+        ("seg_e", _vp * 3), ("seg_ds", _vp * 3), ("seg0", ctypes.c_int), ("nseg", ctypes.c_int),
     ]
 
 

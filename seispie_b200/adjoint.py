@@ -3,11 +3,11 @@
 
 The forward is the fused step (``fwi_run``); the backward is its exact
 discrete transpose (``fwi_run_transposed``), which needs, for every step, the
-forward velocity after the step and the stress divergence of the step.  Those
-are recomputed segment by segment from checkpoints of the full wavefield
-taken every ``K`` steps during the forward pass (uniform checkpointing): the
-memory is ``nt/K`` wavefield copies plus ``K`` steps of velocity and
-divergence, the cost one extra forward sweep.  ``K`` defaults to the value
+strain of the forward velocity after the step and the stress divergence of
+the step.  Those are recomputed segment by segment from checkpoints of the
+full wavefield taken every ``K`` steps during the forward pass (uniform
+checkpointing): the memory is ``nt/K`` wavefield copies plus ``K`` steps of
+strain and divergence, the cost one extra forward sweep.  ``K`` defaults to the value
 that balances the two, shrunk further to fit the memory budget.
 
 The reference's own adjoint (solver.py:290-329) is a subsampled continuous
@@ -27,11 +27,16 @@ from ._lib import FWI_PSV, FWI_SH
 from .engine import COMP, NS, NV, DeviceModel, Grid, ShotBatch, adjoint_injection_lists, injection_lists
 
 
+def strain_fields(mode: int) -> int:
+    """Strain fields stored per step for the gradient (SH exy, ezy; P-SV exx, ezz, exz+ezx)."""
+    return 2 if mode == FWI_SH else 3
+
+
 def default_segment(nt: int, mode: int, nshots: int, grid: Grid, budget_bytes: float | None = None) -> int:
     """Segment length K minimising checkpoint + segment memory
-    (nt/K * (NS+2NV) fields + K * 2NV fields), then shrunk to the budget."""
+    (nt/K * (NS+2NV) fields + K * (NE+NV) fields), then shrunk to the budget."""
     state = NS[mode] + 2 * NV[mode]
-    per_step = 2 * NV[mode]
+    per_step = strain_fields(mode) + NV[mode]
     k = max(1, int(round(math.sqrt(nt * state / per_step))))
     if budget_bytes:
         field = 4 * nshots * grid.nx * grid.pitch
@@ -59,10 +64,11 @@ class ExactAdjoint:
         shape = (self.nshots, g.nx, g.pitch)
         nstate = len(self.fwd.state_tensors())
         self.ckpt = torch.empty((self.nseg, nstate) + shape, dtype=torch.float32, device=dev)
-        self.seg_v = [None, None, None]
+        self.seg_e = [None, None, None]
         self.seg_ds = [None, None, None]
+        for k in range(strain_fields(self.mode)):
+            self.seg_e[k] = torch.empty((self.K,) + shape, dtype=torch.float32, device=dev)
         for c in COMP[self.mode][: NV[self.mode]]:
-            self.seg_v[c] = torch.empty((self.K,) + shape, dtype=torch.float32, device=dev)
             self.seg_ds[c] = torch.empty((self.K,) + shape, dtype=torch.float32, device=dev)
 
     def forward(self) -> list:
@@ -99,9 +105,9 @@ class ExactAdjoint:
             s0, n = s * self.K, min(self.K, self.nt - s * self.K)
             for q, t in enumerate(fwd.state_tensors()):
                 t.copy_(self.ckpt[s, q])
-            fwd.set_segment(self.fdesc, self.seg_v, self.seg_ds, s0, n)
+            fwd.set_segment(self.fdesc, self.seg_e, self.seg_ds, s0, n)
             fwd.run(self.fdesc, False, s0, n)
-            adj.set_segment(adesc, self.seg_v, self.seg_ds, s0, n)
+            adj.set_segment(adesc, self.seg_e, self.seg_ds, s0, n)
             adj.run_transposed(adesc, s0 + n, n)
         fwd.set_segment(self.fdesc, [None] * 3, [None] * 3, 0, 0)
         return tuple(k)

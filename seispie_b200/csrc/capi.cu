@@ -234,8 +234,8 @@ int fwi_run_transposed(fwi_batch *b, int it_hi, int nsteps, void *stream) {
             "fwi_run_transposed: steps [%d, %d) not stored in the segment [%d, %d)", it_hi - nsteps, it_hi, b->seg0,
             b->seg0 + b->nseg);
     const int cx = b->mode == FWI_SH ? 1 : 0;
-    REQUIRE(b->seg_v[cx] && b->seg_ds[cx] && (b->mode == FWI_SH || (b->seg_v[2] && b->seg_ds[2])),
-            "fwi_run_transposed: the segment stores seg_v / seg_ds are required");
+    REQUIRE(b->seg_e[0] && b->seg_e[1] && b->seg_ds[cx] && (b->mode == FWI_SH || (b->seg_e[2] && b->seg_ds[2])),
+            "fwi_run_transposed: the segment stores seg_e / seg_ds are required");
     REQUIRE(b->k_mu, "fwi_run_transposed: k_mu is required");
     if (b->inj_ptr) {
         REQUIRE(b->inj_cell && b->inj_row, "inj_cell and inj_row are required with inj_ptr");

@@ -37,6 +37,8 @@
 // outside the grid or in row padding ever reaches a result.
 #include <cooperative_groups.h>
 
+#include <type_traits>
+
 #include <cstdio>
 
 #include "common.cuh"
@@ -87,7 +89,8 @@ struct StepArgs {
     float *obs[3];
     float *snap_u[3];  // already offset to the slot, or NULL
     float *snap_v[3];
-    float *seg_v[3];   // per-step store of the new velocity (exact adjoint), slot-offset, or NULL
+    float *seg_e[3];   // per-step store of the strain of the new velocity (exact adjoint): SH exy, ezy |
+                       // P-SV exx, ezz, exz+ezx; slot-offset, or NULL
     float *seg_ds[3];  // per-step store of the stress divergence incl. sources, or NULL
 };
 
@@ -382,16 +385,25 @@ __device__ __forceinline__ void stress_update(const StepArgs &a, const float *s0
     constexpr int FS = T::FS, FI = TX * TZ;
     const float dt = a.dt;
     if (MODE == FWI_SH) {
-        const float dm = dt * ip[0];
-        a.sig_out[0][g] = s0[0] + dm * dxp(0);
-        a.sig_out[1][g] = s0[FS] + dm * dzp(0);
+        const float dm = dt * ip[0], exy = dxp(0), ezy = dzp(0);
+        a.sig_out[0][g] = s0[0] + dm * exy;
+        a.sig_out[1][g] = s0[FS] + dm * ezy;
+        if (a.seg_e[0]) {
+            a.seg_e[0][g] = exy;
+            a.seg_e[1][g] = ezy;
+        }
     } else {
         const float lam = ip[0], mu = ip[FI];
         const float vxx = dxp(0), vxz = dzp(0), vzx = dxp(1), vzz = dzp(1);
-        const float l2m = lam + 2.f * mu;
+        const float l2m = lam + 2.f * mu, shear = vxz + vzx;
         a.sig_out[0][g] = s0[0] + dt * (l2m * vxx + lam * vzz);
         a.sig_out[1][g] = s0[FS] + dt * (l2m * vzz + lam * vxx);
-        a.sig_out[2][g] = s0[2 * FS] + dt * (mu * (vxz + vzx));
+        a.sig_out[2][g] = s0[2 * FS] + dt * (mu * shear);
+        if (MODE == FWI_PSV && a.seg_e[0]) {
+            a.seg_e[0][g] = vxx;
+            a.seg_e[1][g] = vzz;
+            a.seg_e[2][g] = shear;
+        }
         if (MODE == FWI_SPIN) {
             const float nu = ip[2 * FI], mnc = ip[3 * FI];
             a.sig_out[4][g] = s0[4 * FS] + a.dt2 * nu * (-vyc - 0.5f * (vzx - vxz));
@@ -414,7 +426,6 @@ __device__ __forceinline__ void store_interior(const StepArgs &a, const Smem<MOD
         a.disp[q][g] = u;
         if (a.snap_u[q]) a.snap_u[q][g] = u;
         if (a.snap_v[q]) a.snap_v[q][g] = v[q];
-        if (a.seg_v[q]) a.seg_v[q][g] = v[q];
         if (a.seg_ds[q]) a.seg_ds[q][g] = ds[q];
     }
 }
@@ -893,9 +904,14 @@ int launch_step(const fwi_batch *b, int adjoint, int it, bool snap_u_next, int s
                                                                           : nullptr;
         a.snap_v[q] = (on && !adjoint && snap_v && b->snap_v[slot]) ? b->snap_v[slot] + snap_v_slot * field
                                                                      : nullptr;
-        const bool seg = on && !adjoint && it - b->seg0 >= 0 && it - b->seg0 < b->nseg;
-        a.seg_v[q] = (seg && b->seg_v[slot]) ? b->seg_v[slot] + (long long)(it - b->seg0) * field : nullptr;
+        const bool seg = on && !adjoint && b->mode != FWI_SPIN && it - b->seg0 >= 0 && it - b->seg0 < b->nseg;
         a.seg_ds[q] = (seg && b->seg_ds[slot]) ? b->seg_ds[slot] + (long long)(it - b->seg0) * field : nullptr;
+    }
+    {
+        const bool seg = !adjoint && b->mode != FWI_SPIN && it - b->seg0 >= 0 && it - b->seg0 < b->nseg;
+        const int ne = b->mode == FWI_SH ? 2 : 3;
+        for (int k = 0; k < 3; k++)
+            a.seg_e[k] = (seg && k < ne && b->seg_e[k]) ? b->seg_e[k] + (long long)(it - b->seg0) * field : nullptr;
     }
     if (b->mode == FWI_SH) {
         a.stf[0] = b->stf[1];
@@ -931,7 +947,7 @@ static void forward_args(const fwi_batch *b, int cur, StepArgs &a) {
         a.vel_out[q] = on ? b->vel[nxt][q] : nullptr;
         a.disp[q] = on ? b->disp[q] : nullptr;
         a.obs[q] = on ? b->obs[comp_slot(b->mode, q)] : nullptr;
-        a.snap_u[q] = a.snap_v[q] = a.seg_v[q] = a.seg_ds[q] = nullptr;
+        a.snap_u[q] = a.snap_v[q] = a.seg_e[q] = a.seg_ds[q] = nullptr;
     }
     if (b->mode == FWI_SH) {
         a.stf[0] = b->stf[1];
@@ -1080,17 +1096,20 @@ int multi_run(fwi_batch *const *bs, int n, void *ws, int it0, int nsteps, cudaSt
 //   dL/dlam = sum dt (sxx~+szz~)(exx+ezz),
 //   dL/dmu  = sum dt (2 sxx~ exx + 2 szz~ ezz + sxz~ (exz+ezx))  [SH: dt (sxy~ exy + szy~ ezy)]
 //   dL/db   = sum v~' . d
-// (sig~ before the step; e = D+ of the forward v', v' and d stored per step
-// by a recomputed forward segment).
+// (sig~ before the step; e = D+ of the forward v' and d are stored per step,
+// pointwise, by a recomputed forward segment).
 //
 // Mapping.  A cluster of C <= 8 CTAs owns one 32 x 32 tile; CTA r of the
 // cluster processes shots r, r+C, ... in turn, keeping the model tile
 // (stiffness with halo, dt/rho, sponge) in shared memory across its shots
-// and its gradient terms in registers.  Per shot it stages sig~, v~ and the
-// forward v' with TMA, forms t = dt S^T sig~ in place, computes v~' on the
-// interior (lane = z, x taps in a register window, as step_kernel_rw) plus
-// the halo, then sig~' and the gradient terms of the interior.  At the end
-// the cluster sums its CTAs' terms through distributed shared memory in
+// and its gradient terms in registers.  Per shot it forms t = dt S^T sig~ in
+// place over the staged sig~, computes v~' on the interior (lane = z, x taps
+// in a register window, as step_kernel_rw) plus the halo, then sig~' and the
+// gradient terms of the interior.  Staging is pipelined with TMA: the next
+// shot's sig~ streams in as soon as t has been consumed, its v~ and strain
+// once the stress half is done (the injection waits for v~ only after t has
+// been formed, so that copy overlaps the t pass).  At the
+// end the cluster sums its CTAs' terms through distributed shared memory in
 // rank order and adds them once into the FP64 gradient arrays: one
 // read-modify-write per cell and step for all shots, deterministic, no
 // atomics.
@@ -1101,16 +1120,17 @@ struct AdjArgs {
     float cx1, cx2, cz1, cz2, dt;
     float *sig_out[3];
     float *vel_out[2];
-    const float *dsf[2];   // forward divergence of step it, per component
-    double *k[3];          // SH: dL/dmu, dL/dbuo | P-SV: dL/dlam, dL/dmu, dL/dbuo ([nx][pitch], NULL skips)
+    const float *dsf[2];  // forward divergence of step it, per velocity component
+    const float *ef[3];   // forward strain of v(it+1): SH exy, ezy | P-SV exx, ezz, exz+ezx
+    double *k[3];         // SH: dL/dmu, dL/dbuo | P-SV: dL/dlam, dL/dmu, dL/dbuo ([nx][pitch], NULL skips)
     const int *inj_ptr, *inj_cell, *inj_row;
-    const float *g[2];     // u~ at the receivers per step (forward time order)
+    const float *g[2];    // u~ at the receivers per step (forward time order)
 };
 
 struct AdjMaps {
     CUtensorMap sig[3];  // sig~, stress region box
     CUtensorMap vel[2];  // v~, velocity region box
-    CUtensorMap vf[2];   // forward v(it+1), velocity region box
+    CUtensorMap ef[3];   // forward strain, interior box
     CUtensorMap lm[2];   // SH: mu | P-SV: lam, mu; stress region box
     CUtensorMap vp[2];   // dt/rho, sponge; velocity region box
 };
@@ -1123,18 +1143,21 @@ struct AdjTile {
     static constexpr int FS = (SX * SZ + 31) / 32 * 32, FV = (VX * SZ + 31) / 32 * 32;
     static constexpr int NL = MODE == FWI_SH ? 1 : 2;  // stiffness fields
     static constexpr int NK = MODE == FWI_SH ? 2 : 3;  // gradient fields
-    // per-shot region (sig~, v~, forward v'), then the model tile, the
-    // injection list and two mbarriers (model, shot)
-    static constexpr int V_OFF = F::NS * FS, VF_OFF = V_OFF + F::NV * FV;
-    static constexpr int L_OFF = VF_OFF + F::NV * FV, P_OFF = L_OFF + NL * FS;
+    static constexpr int NE = MODE == FWI_SH ? 2 : 3;  // forward strain fields
+    // sig~ (turned into t in place), v~, the forward strain of the interior,
+    // the model tile, the injection list and three mbarriers (model, sig~,
+    // v~ with strain)
+    static constexpr int V_OFF = F::NS * FS, E_OFF = V_OFF + F::NV * FV;
+    static constexpr int L_OFF = E_OFF + NE * TX * TZ, P_OFF = L_OFF + NL * FS;
     static constexpr int LIST_OFF = P_OFF + 2 * FV;
     static constexpr int LIST = kThreads * (1 + F::NINJ) + 8;
     static constexpr int BAR_OFF = (LIST_OFF + LIST + 1) / 2 * 2;
-    static constexpr size_t bytes = sizeof(float) * (size_t)(BAR_OFF + 4);
-    static constexpr uint32_t shot_bytes = 4u * (F::NS * SX * SZ + 2 * F::NV * VX * SZ);
+    static constexpr size_t bytes = sizeof(float) * (size_t)(BAR_OFF + 8);
+    static constexpr uint32_t sig_bytes = 4u * F::NS * SX * SZ;
+    static constexpr uint32_t vel_bytes = 4u * (F::NV * VX * SZ + NE * TX * TZ);
     static constexpr uint32_t model_bytes = 4u * (NL * SX * SZ + 2 * VX * SZ);
-    static_assert(NK * TX * TZ <= L_OFF, "gradient terms overlay the per-shot region");
-    static_assert(shot_bytes < (1u << 20) && model_bytes < (1u << 20), "mbarrier transaction count limit");
+    static_assert(NK * TX * TZ <= L_OFF, "gradient terms overlay the per-shot buffers");
+    static_assert(vel_bytes < (1u << 20) && model_bytes < (1u << 20), "mbarrier transaction count limit");
 };
 
 // Injection of u~ for one shot: entries whose cell lies in the computed
@@ -1195,23 +1218,25 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : 3)
     using T = AdjTile<MODE>;
     using F = Fields<MODE>;
     constexpr int TX = T::TX, TZ = T::TZ, SX = T::SX, SZ = T::SZ, RVZ = T::RVZ, FS = T::FS, FV = T::FV;
-    constexpr int NS = F::NS, NV = F::NV, NL = T::NL, NK = T::NK, RPW = TX / (kThreads / 32);
+    constexpr int NS = F::NS, NV = F::NV, NL = T::NL, NK = T::NK, NE = T::NE, RPW = TX / (kThreads / 32);
     extern __shared__ __align__(128) float smem[];
-    float *sS = smem, *sV = smem + T::V_OFF, *sF = smem + T::VF_OFF, *sL = smem + T::L_OFF, *sP = smem + T::P_OFF;
+    float *sS = smem, *sV = smem + T::V_OFF, *sE = smem + T::E_OFF, *sL = smem + T::L_OFF, *sP = smem + T::P_OFF;
     int *sLoc = reinterpret_cast<int *>(smem + T::LIST_OFF);
     float *sVal = reinterpret_cast<float *>(sLoc + kThreads);
     int *sWarp = reinterpret_cast<int *>(sVal + F::NINJ * kThreads);
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + T::BAR_OFF);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + T::BAR_OFF);  // model, sig~, v~ with strain
     cg::cluster_group cluster = cg::this_cluster();
     const int crank = (int)cluster.block_rank(), csize = (int)cluster.num_blocks();
 
     const int tid = threadIdx.x, lane = tid & 31, ix0 = (tid >> 5) * RPW;
     const int z0 = blockIdx.x * TZ, x0 = blockIdx.y * TX;
-    const int nx = a.nx, nz = a.nz, pitch = a.pitch;
+    const int nx = a.nx, nz = a.nz, pitch = a.pitch, nshots = a.nshots;
     const int gz = z0 + lane, col = lane + 4;
     const bool zin = gz < nz;
     const float dt = a.dt, cx1 = a.cx1, cx2 = a.cx2, cz1 = a.cz1, cz2 = a.cz2;
-    // z masks of this lane: (D+)^T taps gz-2..gz+1, (D-)^T taps gz-1..gz+2
+    // z masks of this lane: (D+)^T taps gz-2..gz+1, (D-)^T taps gz-1..gz+2;
+    // all ones (and skipped) unless the tile reaches a z edge
+    const bool zedge = !(z0 >= 3 && z0 + TZ + 4 <= nz);
     float pz[4], mz[4];
 #pragma unroll
     for (int d = 0; d < 4; d++) {
@@ -1219,11 +1244,26 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : 3)
         pz[d] = (kp >= 1 && kp < nz - 2) ? 1.f : 0.f;
         mz[d] = (km >= 2 && km < nz - 2) ? 1.f : 0.f;
     }
-    const bool okz = gz >= 1 && gz < nz - 2;
 
+    // copies issued by thread 0; each refill of a buffer is ordered after the
+    // generic-proxy accesses that preceded it (the barrier before the call)
+    auto issue_sig = [&](int shot) {
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        mbar_expect_tx(&bar[1], T::sig_bytes);
+#pragma unroll
+        for (int f = 0; f < NS; f++) tma_load_3d(sS + f * FS, &m.sig[f], z0 - 4, x0 - 3, shot, &bar[1]);
+    };
+    auto issue_vel = [&](int shot) {
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        mbar_expect_tx(&bar[2], T::vel_bytes);
+#pragma unroll
+        for (int q = 0; q < NV; q++) tma_load_3d(sV + q * FV, &m.vel[q], z0 - 4, x0 - 1, shot, &bar[2]);
+#pragma unroll
+        for (int k = 0; k < NE; k++) tma_load_3d(sE + k * TX * TZ, &m.ef[k], z0, x0, shot, &bar[2]);
+    };
     if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+#pragma unroll
+        for (int b = 0; b < 3; b++) mbar_init(&bar[b], 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     __syncthreads();
@@ -1233,6 +1273,10 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : 3)
         for (int f = 0; f < NL; f++) tma_load_2d(sL + f * FS, &m.lm[f], z0 - 4, x0 - 3, &bar[0]);
 #pragma unroll
         for (int p = 0; p < 2; p++) tma_load_2d(sP + p * FV, &m.vp[p], z0 - 4, x0 - 1, &bar[0]);
+        if (crank < nshots) {
+            issue_sig(crank);
+            issue_vel(crank);
+        }
     }
 
     float gk[NK][RPW];
@@ -1241,21 +1285,9 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : 3)
 #pragma unroll
         for (int q = 0; q < RPW; q++) gk[k][q] = 0.f;
 
-    int iter = 0;
-    bool failed = false;
-    for (int shot = crank; shot < a.nshots; shot += csize, iter++) {
+    int i = 0;
+    for (int shot = crank; shot < nshots; shot += csize, i++) {
         const long long soff = (long long)shot * nx * pitch;
-        if (tid == 0) {
-            // the previous shot's generic-proxy accesses of this memory are ordered before the copies
-            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-            mbar_expect_tx(&bar[1], T::shot_bytes);
-#pragma unroll
-            for (int f = 0; f < NS; f++) tma_load_3d(sS + f * FS, &m.sig[f], z0 - 4, x0 - 3, shot, &bar[1]);
-#pragma unroll
-            for (int q = 0; q < NV; q++) tma_load_3d(sV + q * FV, &m.vel[q], z0 - 4, x0 - 1, shot, &bar[1]);
-#pragma unroll
-            for (int q = 0; q < NV; q++) tma_load_3d(sF + q * FV, &m.vf[q], z0 - 4, x0 - 1, shot, &bar[1]);
-        }
         // forward divergence of the interior cells (read once: straight from HBM)
         float dsv[NV][RPW];
 #pragma unroll
@@ -1269,53 +1301,77 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : 3)
         const bool single = p1 - p0 <= kThreads;
         int n_in = 0;
         if (single && p1 > p0) n_in = adj_collect<MODE>(a, p0, p1, x0, z0, sLoc, sVal, sWarp);
-        bool ok = mbar_wait(&bar[1], iter & 1);
-        if (iter == 0) ok = mbar_wait(&bar[0], 0) && ok;
+
+        // sig~ of the interior cells into registers (t overwrites it)
+        bool ok = mbar_wait(&bar[1], i & 1);
+        if (i == 0) ok = mbar_wait(&bar[0], 0) && ok;
+        float sg[NS][RPW];
+#pragma unroll
+        for (int f = 0; f < NS; f++)
+#pragma unroll
+            for (int q = 0; q < RPW; q++) sg[f][q] = sS[f * FS + (ix0 + q + 3) * SZ + col];
         if (__syncthreads_or(!ok)) {  // block-uniform decision
             if (tid == 0) atomicExch(&g_device_status, 1);
-            mbar_wait(&bar[1], iter & 1);  // one more bounded chance for copies in flight
-            if (iter == 0) mbar_wait(&bar[0], 0);
-            failed = true;
+            // one more bounded chance for every copy in flight to land
+            mbar_wait(&bar[1], i & 1);
+            mbar_wait(&bar[2], i & 1);
+            if (i == 0) mbar_wait(&bar[0], 0);
             break;
         }
-        if (single) {
-            adj_apply<MODE>(sV, n_in, sLoc, sVal, dt);
-        } else {
+        // t = dt S^T sig~ in place over the whole stress region, four cells
+        // (one 16-byte vector) at a time
+        for (int c = tid; c < SX * (SZ / 4); c += kThreads) {
+            float4 *s4 = reinterpret_cast<float4 *>(sS) + c;
+            const float4 *l4 = reinterpret_cast<const float4 *>(sL) + c;
+            constexpr int F4 = FS / 4;
+            if (MODE == FWI_SH) {
+                const float4 mu = l4[0];
+                float4 a0 = s4[0], a1 = s4[F4];
+                a0.x = dt * (mu.x * a0.x); a0.y = dt * (mu.y * a0.y); a0.z = dt * (mu.z * a0.z); a0.w = dt * (mu.w * a0.w);
+                a1.x = dt * (mu.x * a1.x); a1.y = dt * (mu.y * a1.y); a1.z = dt * (mu.z * a1.z); a1.w = dt * (mu.w * a1.w);
+                s4[0] = a0;
+                s4[F4] = a1;
+            } else {
+                const float4 l = l4[0], mu = l4[F4];
+                float4 xx = s4[0], zz = s4[F4], xz = s4[2 * F4];
+                auto t3 = [&](float lc, float mc, float &sxx, float &szz, float &sxz) {
+                    const float l2m = lc + 2.f * mc, a = sxx, b = szz;
+                    sxx = dt * (l2m * a + lc * b);
+                    szz = dt * (lc * a + l2m * b);
+                    sxz = dt * (mc * sxz);
+                };
+                t3(l.x, mu.x, xx.x, zz.x, xz.x);
+                t3(l.y, mu.y, xx.y, zz.y, xz.y);
+                t3(l.z, mu.z, xx.z, zz.z, xz.z);
+                t3(l.w, mu.w, xx.w, zz.w, xz.w);
+                s4[0] = xx;
+                s4[F4] = zz;
+                s4[2 * F4] = xz;
+            }
+        }
+        // v~ and the forward strain of this shot; u~ enters v~ (thread 0)
+        ok = mbar_wait(&bar[2], i & 1);
+        if (single && ok) adj_apply<MODE>(sV, n_in, sLoc, sVal, dt);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicExch(&g_device_status, 1);
+            mbar_wait(&bar[2], i & 1);
+            break;
+        }
+        if (!single) {
             for (int base = p0; base < p1; base += kThreads) {
                 __syncthreads();
                 const int n = adj_collect<MODE>(a, base, p1, x0, z0, sLoc, sVal, sWarp);
                 __syncthreads();
                 adj_apply<MODE>(sV, n, sLoc, sVal, dt);
             }
+            __syncthreads();
         }
-        // sig~ of the interior cells into registers (t overwrites it)
-        float sg[NS][RPW];
-#pragma unroll
-        for (int f = 0; f < NS; f++)
-#pragma unroll
-            for (int q = 0; q < RPW; q++) sg[f][q] = sS[f * FS + (ix0 + q + 3) * SZ + col];
-        __syncthreads();
-        // t = dt S^T sig~ in place, stress region rows, columns z0-3 .. z0+TZ+2
-        for (int c = tid; c < SX * (SZ - 2); c += kThreads) {
-            const int r = c / (SZ - 2), i = r * SZ + (c - r * (SZ - 2)) + 1;
-            if (MODE == FWI_SH) {
-                const float mu = sL[i];
-                sS[i] = dt * (mu * sS[i]);
-                sS[FS + i] = dt * (mu * sS[FS + i]);
-            } else {
-                const float l = sL[i], mu = sL[FS + i], l2m = l + 2.f * mu;
-                const float sxx = sS[i], szz = sS[FS + i], sxz = sS[2 * FS + i];
-                sS[i] = dt * (l2m * sxx + l * szz);
-                sS[FS + i] = dt * (l * sxx + l2m * szz);
-                sS[2 * FS + i] = dt * (mu * sxz);
-            }
-        }
-        __syncthreads();
 
         // ---- v~' on the warp's interior rows; t rows x-2 .. x+1 of the
         // x-differentiated fields in a register window, pre-masked
         // (window index r <-> stress row ix0+1+r <-> grid row x0+ix0-2+r)
-        {
+        auto vel_interior = [&](auto zm) {
+            constexpr bool ZM = decltype(zm)::value;  // z masks needed (tile at a z edge)
             float w[NS][RPW + 3];
 #pragma unroll
             for (int f = 0; f < NS; f++)
@@ -1341,7 +1397,10 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : 3)
                 };
                 auto dzpT = [&](int f) -> float {
                     const float *t = trow + f * FS;
-                    return cz1 * (t[-1] * pz[1] - t[0] * pz[2]) - cz2 * (t[-2] * pz[0] - t[1] * pz[3]);
+                    if constexpr (ZM)
+                        return cz1 * (t[-1] * pz[1] - t[0] * pz[2]) - cz2 * (t[-2] * pz[0] - t[1] * pz[3]);
+                    else
+                        return cz1 * (t[-1] - t[0]) - cz2 * (t[-2] - t[1]);
                 };
                 float acc[2];
                 if (MODE == FWI_SH) {
@@ -1362,7 +1421,9 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : 3)
                 }
                 gk[NK - 1][q] += gb;
             }
-        }
+        };
+        if (zedge) vel_interior(std::true_type{});
+        else vel_interior(std::false_type{});
         // ---- v~' on the halo rows x0-1, x0+TX, x0+TX+1 and columns z0-1,
         // z0+TZ, z0+TZ+1 (redundant with the neighbour tiles; masks per tap)
         {
@@ -1409,60 +1470,62 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : 3)
             }
         }
         __syncthreads();
+        // t has been consumed: the next shot's sig~ streams in during the stress half
+        if (tid == 0 && shot + csize < nshots) issue_sig(shot + csize);
 
         // ---- sig~' and the stiffness gradient terms on the interior; b v~'
-        // (pre-masked) and the forward v' rows x-1 .. x+2 in register windows
+        // rows x-1 .. x+2 in a register window, pre-masked
         // (window index r <-> velocity row ix0+r <-> grid row x0+ix0-1+r)
-        {
-            float w[NV][RPW + 3], f[NV][RPW + 3];
+        auto stress_interior = [&](auto zm) {
+            constexpr bool ZM = decltype(zm)::value;
+            float w[NV][RPW + 3];
 #pragma unroll
             for (int c = 0; c < NV; c++) {
 #pragma unroll
                 for (int r = 0; r < RPW + 3; r++) {
                     const int gr = x0 + ix0 - 1 + r;
                     w[c][r] = (gr >= 2 && gr < nx - 2) ? sV[c * FV + (ix0 + r) * SZ + col] : 0.f;
-                    f[c][r] = sF[c * FV + (ix0 + r) * SZ + col];
                 }
             }
 #pragma unroll
             for (int q = 0; q < RPW; q++) {
                 const int ix = ix0 + q, gx = x0 + ix;
                 if (!(zin && gx < nx)) continue;
-                const bool okx = gx >= 1 && gx < nx - 2;
-                const float *vrow = sV + (ix + 1) * SZ + col, *frow = sF + (ix + 1) * SZ + col;
+                const float *vrow = sV + (ix + 1) * SZ + col;
+                const float *e = sE + ix * TZ + lane;
                 auto dxmT = [&](int c) -> float {
                     return cx1 * (w[c][q + 1] - w[c][q + 2]) - cx2 * (w[c][q] - w[c][q + 3]);
                 };
                 auto dzmT = [&](int c) -> float {
                     const float *v = vrow + c * FV;
-                    return cz1 * (v[0] * mz[1] - v[1] * mz[2]) - cz2 * (v[-1] * mz[0] - v[2] * mz[3]);
-                };
-                auto dxp = [&](int c) -> float {
-                    return okx ? cx1 * (f[c][q + 2] - f[c][q + 1]) - cx2 * (f[c][q + 3] - f[c][q]) : 0.f;
-                };
-                auto dzp = [&](int c) -> float {
-                    const float *v = frow + c * FV;
-                    return okz ? cz1 * (v[1] - f[c][q + 1]) - cz2 * (v[2] - v[-1]) : 0.f;
+                    if constexpr (ZM)
+                        return cz1 * (v[0] * mz[1] - v[1] * mz[2]) - cz2 * (v[-1] * mz[0] - v[2] * mz[3]);
+                    else
+                        return cz1 * (v[0] - v[1]) - cz2 * (v[-1] - v[2]);
                 };
                 const long long g = soff + (long long)gx * pitch + gz;
                 if (MODE == FWI_SH) {
                     a.sig_out[0][g] = sg[0][q] + dxmT(0);
                     a.sig_out[1][g] = sg[1][q] + dzmT(0);
-                    gk[0][q] += dt * (sg[0][q] * dxp(0) + sg[1][q] * dzp(0));
+                    gk[0][q] += dt * (sg[0][q] * e[0] + sg[1][q] * e[TX * TZ]);
                 } else {
                     a.sig_out[0][g] = sg[0][q] + dxmT(0);
                     a.sig_out[1][g] = sg[1][q] + dzmT(1);
                     a.sig_out[2][g] = sg[2][q] + (dzmT(0) + dxmT(1));
-                    const float exx = dxp(0), exz = dzp(0), ezx = dxp(1), ezz = dzp(1);
                     const float sxx = sg[0][q], szz = sg[1][q], sxz = sg[2][q];
+                    const float exx = e[0], ezz = e[TX * TZ];
                     gk[0][q] += dt * ((sxx + szz) * (exx + ezz));
-                    gk[1][q] += dt * (2.f * (sxx * exx + szz * ezz) + sxz * (exz + ezx));
+                    gk[1][q] += dt * (2.f * (sxx * exx + szz * ezz) + sxz * e[2 * TX * TZ]);
                 }
             }
-        }
-        __syncthreads();  // shared memory is refilled for the next shot
+        };
+        if (zedge) stress_interior(std::true_type{});
+        else stress_interior(std::false_type{});
+        __syncthreads();
+        // v~ and strain buffers are free: the next shot streams into them
+        if (tid == 0 && shot + csize < nshots) issue_vel(shot + csize);
     }
-    if (iter == 0 && !failed) mbar_wait(&bar[0], 0);  // no shot: let the model copies land
+    if (crank >= nshots) mbar_wait(&bar[0], 0);  // no shot: let the model copies land
 
     // ---- cluster sum of the gradient terms, in rank order, into FP64
     float *part = smem;
@@ -1486,14 +1549,14 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : 3)
 
 // Tensor maps of one transposed step.
 template <int MODE>
-static int adjoint_maps(const fwi_batch *b, const float *const *vf, AdjMaps &m) {
+static int adjoint_maps(const fwi_batch *b, const AdjArgs &a, AdjMaps &m) {
     using T = AdjTile<MODE>;
     using F = Fields<MODE>;
     const int cur = b->cur, nx = b->nx, pitch = b->pitch, ns = b->nshots;
     int rc = 0;
     for (int f = 0; f < F::NS && !rc; f++) rc = encode_map(&m.sig[f], b->sig[cur][f], 3, pitch, nx, ns, T::SZ, T::SX);
     for (int q = 0; q < F::NV && !rc; q++) rc = encode_map(&m.vel[q], b->vel[cur][q], 3, pitch, nx, ns, T::SZ, T::VX);
-    for (int q = 0; q < F::NV && !rc; q++) rc = encode_map(&m.vf[q], vf[q], 3, pitch, nx, ns, T::SZ, T::VX);
+    for (int k = 0; k < T::NE && !rc; k++) rc = encode_map(&m.ef[k], a.ef[k], 3, pitch, nx, ns, T::TZ, T::TX);
     const float *lm[2] = {MODE == FWI_SH ? b->mu : b->lam, b->mu};
     for (int f = 0; f < T::NL && !rc; f++) rc = encode_map(&m.lm[f], lm[f], 2, pitch, nx, 1, T::SZ, T::SX);
     const float *vp[2] = {b->buo, b->bound};
@@ -1501,11 +1564,25 @@ static int adjoint_maps(const fwi_batch *b, const float *const *vf, AdjMaps &m) 
     return rc;
 }
 
-// Shots per cluster of the transposed step (portable cluster size limit 8).
-static int adjoint_cluster(int nshots) { return nshots < 8 ? nshots : 8; }
+// Shots processed side by side per tile (the cluster size, portable limit
+// 8): every CTA pays one cluster reduction, so the fewest CTAs that still
+// give about 2.5 waves of the resident-CTA slots (measured on 512 x 512 x 32
+// shots: 4 beats 2, 8 and 16).
+static int adjoint_cluster(int nshots, long long tiles, int ctas_per_sm) {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+            sms = 148;
+    }
+    int c = 8;
+    while (c > 1 && tiles * c * 2 > 5ll * sms * ctas_per_sm) c /= 2;
+    return c < nshots ? c : nshots;
+}
 
 template <int MODE>
-static int launch_adjoint(const fwi_batch *b, const AdjArgs &a, const float *const *vf, cudaStream_t st) {
+static int launch_adjoint(const fwi_batch *b, const AdjArgs &a, cudaStream_t st) {
     using T = AdjTile<MODE>;
     static bool set = false;
     if (!set) {
@@ -1515,9 +1592,10 @@ static int launch_adjoint(const fwi_batch *b, const AdjArgs &a, const float *con
         set = true;
     }
     AdjMaps m;
-    int rc = adjoint_maps<MODE>(b, vf, m);
+    int rc = adjoint_maps<MODE>(b, a, m);
     if (rc) return rc;
-    const int C = adjoint_cluster(b->nshots);
+    const int C = adjoint_cluster(b->nshots, (long long)((b->nz + T::TZ - 1) / T::TZ) * ((b->nx + T::TX - 1) / T::TX),
+                                  MODE == FWI_SH ? 4 : 3);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((b->nz + T::TZ - 1) / T::TZ, (b->nx + T::TX - 1) / T::TX, C);
     cfg.blockDim = dim3(kThreads, 1, 1);
@@ -1552,14 +1630,13 @@ int launch_adjoint_step(const fwi_batch *b, int it, cudaStream_t st) {
     a.cz2 = (float)(1.0 / (24.0 * (double)b->dz));
     a.dt = (float)b->dt;
     const bool sh = b->mode == FWI_SH;
-    const int nxt = 1 - b->cur, ns = sh ? 2 : 3, nv = sh ? 1 : 2;
+    const int nxt = 1 - b->cur, ns = sh ? 2 : 3, nv = sh ? 1 : 2, ne = sh ? 2 : 3;
     for (int f = 0; f < 3; f++) a.sig_out[f] = f < ns ? b->sig[nxt][f] : nullptr;
     for (int q = 0; q < 2; q++) a.vel_out[q] = q < nv ? b->vel[nxt][q] : nullptr;
     const long long field = (long long)b->nshots * b->nx * b->pitch;
     const long long slot = it - b->seg0;
-    const int cx = sh ? 1 : 0;
-    const float *vf[2] = {b->seg_v[cx] + slot * field, sh ? nullptr : b->seg_v[2] + slot * field};
-    a.dsf[0] = b->seg_ds[cx] + slot * field;
+    for (int k = 0; k < 3; k++) a.ef[k] = k < ne ? b->seg_e[k] + slot * field : nullptr;
+    a.dsf[0] = b->seg_ds[sh ? 1 : 0] + slot * field;
     a.dsf[1] = sh ? nullptr : b->seg_ds[2] + slot * field;
     if (sh) {
         a.k[0] = b->k_mu;
@@ -1575,7 +1652,7 @@ int launch_adjoint_step(const fwi_batch *b, int it, cudaStream_t st) {
     a.inj_row = b->inj_row;
     a.g[0] = sh ? b->stf[1] : b->stf[0];
     a.g[1] = sh ? nullptr : b->stf[2];
-    return sh ? launch_adjoint<FWI_SH>(b, a, vf, st) : launch_adjoint<FWI_PSV>(b, a, vf, st);
+    return sh ? launch_adjoint<FWI_SH>(b, a, st) : launch_adjoint<FWI_PSV>(b, a, st);
 }
 
 }  // namespace fwi

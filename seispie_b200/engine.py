@@ -214,10 +214,11 @@ class ShotBatch:
         b.k_lam, b.k_mu, b.k_rho = (ptr(k) for k in kernels)
         return b
 
-    def set_segment(self, b: FwiBatch, seg_v, seg_ds, seg0: int, nseg: int) -> FwiBatch:
-        """Point a descriptor at per-step segment stores (exact adjoint)."""
+    def set_segment(self, b: FwiBatch, seg_e, seg_ds, seg0: int, nseg: int) -> FwiBatch:
+        """Point a descriptor at per-step segment stores (exact adjoint):
+        strain fields seg_e[k] and divergence per component slot seg_ds[c]."""
         for c in range(3):
-            b.seg_v[c] = ptr(seg_v[c])
+            b.seg_e[c] = ptr(seg_e[c])
             b.seg_ds[c] = ptr(seg_ds[c])
         b.seg0, b.nseg = int(seg0), int(nseg)
         return b
