@@ -273,6 +273,70 @@ int fwi_misfit_noalloc(const float *data, const float *syn, float *adstf, double
 int fwi_smooth(const double *in, int in_pitch, float *out, int out_pitch, double *tmp,
                int nx, int nz, int sigma, void *stream);
 
+/*
+ * Learned preconditioner: kernels of a small U-Net (training and inference).
+ * No counterpart in the reference, which has no learned component.
+ * Activations are NHWC bf16 ([n][h][w][c], c a multiple of 16, 16-byte
+ * aligned); 3x3 weights [9][cout][cin] bf16 (tap = 3*(dy+1)+(dx+1), input
+ * channel innermost); biases and gradients FP32.  Arithmetic: bf16 products,
+ * FP32 accumulation on the tensor cores.
+ */
+
+/* out = act(conv3x3(concat(in0, in1), w) + bias), zero padding; channel
+ * counts c0, c1 (c1 = 0: in1 unused), cout = d0 + d1 output channels split
+ * between out0 (first d0) and out1; bias may be NULL; relu != 0 applies
+ * max(., 0).  The data gradient of a layer is this call on the gradient of
+ * its output, with the weights of fwi_unet_flip_weights, no bias and no
+ * relu, splitting the result back into the layer's two inputs. */
+int fwi_unet_conv3x3(const void *in0, int c0, const void *in1, int c1, const void *w, const float *bias,
+                     int cout, void *out0, int d0, void *out1, int d1, int n, int h, int wd, int relu,
+                     void *stream);
+
+/* wd[8-tap][ci][co] = w[tap][co][ci]: the weights of the data gradient. */
+int fwi_unet_flip_weights(const void *w, void *wd, int cout, int cin, void *stream);
+
+/* g[i] = 0 where y[i] <= 0 (gradient through a ReLU whose output is y). */
+int fwi_unet_relu_bwd(void *g, const void *y, long long count, void *stream);
+
+/* Weight and bias gradients of a 3x3 layer: dw[9][cout][c0+c1] = sum over
+ * pixels of g (x) shifted input, db[cout] = sum over pixels of g (db may be
+ * NULL), both summed in a fixed block order.  part: caller scratch of
+ * fwi_unet_wgrad_partials(cout, c0+c1, n, h, w) floats. */
+long long fwi_unet_wgrad_partials(int cout, int cin, int n, int h, int w);
+int fwi_unet_conv3x3_wgrad(const void *g, int cout, const void *in0, int c0, const void *in1, int c1, int n,
+                           int h, int wd, float *part, float *dw, float *db, void *stream);
+
+/* 2x2 average pooling [n][h][w][c] -> [n][h/2][w/2][c] (h, w even) and its
+ * adjoint (accumulate != 0 adds into gin); nearest 2x upsampling
+ * [n][h][w][c] -> [n][2h][2w][c] and its adjoint (h, w of the smaller
+ * image). */
+int fwi_unet_pool2(const void *in, void *out, int c, int n, int h, int w, void *stream);
+int fwi_unet_pool2_bwd(const void *gout, void *gin, int c, int n, int h, int w, int accumulate, void *stream);
+int fwi_unet_up2(const void *in, void *out, int c, int n, int h, int w, void *stream);
+int fwi_unet_up2_bwd(const void *gout, void *gin, int c, int n, int h, int w, void *stream);
+
+/* 1x1 output head from 16 channels: out[p] = sum_c w[c] x[p][c] + b[0]
+ * (FP32), and its adjoint: gx = w gout, gwb[0..15] = dL/dw, gwb[16] = dL/db;
+ * part: caller scratch of 17 * ceil(n*h*w / 4096) floats. */
+int fwi_unet_head(const void *x, const float *w, const float *b, float *out, int n, int h, int wd, void *stream);
+int fwi_unet_head_bwd(const void *x, const float *w, const float *gout, void *gx, float *part, float *gwb, int n,
+                      int h, int wd, void *stream);
+
+/* Network input: three FP32 planes [n][3][h][w] -> [n][h][w][16] bf16, the
+ * channels past the third zero. */
+int fwi_unet_pack(const float *planes, void *x, int n, int h, int w, void *stream);
+
+/* One Adam step on FP32 master weights w with moments m, v and gradient g;
+ * wb (may be NULL) receives the bf16 copy.  step counts from 1. */
+int fwi_unet_adam(float *w, float *m, float *v, const float *g, void *wb, long long count, double lr,
+                  double beta1, double beta2, double eps, int step, void *stream);
+
+/* Mean squared error of out against tgt: *loss (FP64) and gout = dloss/dout.
+ * part: caller scratch of fwi_unet_mse_partials() doubles. */
+long long fwi_unet_mse_partials(void);
+int fwi_unet_mse(const float *out, const float *tgt, float *gout, double *loss, double *part, long long count,
+                 void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -92,6 +92,24 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
                                ctypes.c_int),
         "fwi_smooth": ([_vp, ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp],
                        ctypes.c_int),
+        "fwi_unet_conv3x3": ([_vp, ctypes.c_int, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp,
+                              ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp], ctypes.c_int),
+        "fwi_unet_flip_weights": ([_vp, _vp, ctypes.c_int, ctypes.c_int, _vp], ctypes.c_int),
+        "fwi_unet_relu_bwd": ([_vp, _vp, ctypes.c_longlong, _vp], ctypes.c_int),
+        "fwi_unet_wgrad_partials": ([ctypes.c_int] * 5, ctypes.c_longlong),
+        "fwi_unet_conv3x3_wgrad": ([_vp, ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_int, _vp, _vp, _vp, _vp], ctypes.c_int),
+        "fwi_unet_pool2": ([_vp, _vp] + [ctypes.c_int] * 4 + [_vp], ctypes.c_int),
+        "fwi_unet_pool2_bwd": ([_vp, _vp] + [ctypes.c_int] * 5 + [_vp], ctypes.c_int),
+        "fwi_unet_up2": ([_vp, _vp] + [ctypes.c_int] * 4 + [_vp], ctypes.c_int),
+        "fwi_unet_up2_bwd": ([_vp, _vp] + [ctypes.c_int] * 4 + [_vp], ctypes.c_int),
+        "fwi_unet_head": ([_vp, _vp, _vp, _vp] + [ctypes.c_int] * 3 + [_vp], ctypes.c_int),
+        "fwi_unet_head_bwd": ([_vp] * 6 + [ctypes.c_int] * 3 + [_vp], ctypes.c_int),
+        "fwi_unet_pack": ([_vp, _vp] + [ctypes.c_int] * 3 + [_vp], ctypes.c_int),
+        "fwi_unet_adam": ([_vp, _vp, _vp, _vp, _vp, ctypes.c_longlong, ctypes.c_double, ctypes.c_double,
+                           ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp], ctypes.c_int),
+        "fwi_unet_mse_partials": ([], ctypes.c_longlong),
+        "fwi_unet_mse": ([_vp, _vp, _vp, _vp, _vp, ctypes.c_longlong, _vp], ctypes.c_int),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(lib, name)

@@ -19,7 +19,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 OUT_DIR = os.path.join(PKG, "_build")
 LIB = os.path.join(OUT_DIR, "libseispie_b200.so")
-SOURCES = ("capi.cu", "step.cu", "aux.cu", "linalg.cu", "noalloc.cu")
+SOURCES = ("capi.cu", "step.cu", "aux.cu", "linalg.cu", "noalloc.cu", "unet.cu")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
