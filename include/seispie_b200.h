@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define FWI_ABI_VERSION 3
+#define FWI_ABI_VERSION 4
 
 /* status codes */
 #define FWI_OK 0
@@ -99,16 +99,20 @@ typedef struct fwi_batch {
     float *snap_u[3];
     float *snap_v[3];
     double *k_lam, *k_mu, *k_rho;
-    /* Exact discrete adjoint (fwi_run_transposed).  SH / P-SV forward runs
-     * with these set also store, for every step it with 0 <= it-seg0 < nseg,
-     * at slot it-seg0 of [nseg][nshots][nx][pitch] buffers: the strain of the
-     * new velocity v(it+1) (D+ of it, masked as the stress update uses it)
-     * into seg_e[k] -- SH: exy, ezy; P-SV: exx, ezz, exz+ezx -- and the stress
-     * divergence including the sources of step it into seg_ds[c] (component
-     * slots as obs).  NULL skips. */
-    float *seg_e[3];
+    /* Exact discrete adjoint (fwi_run_transposed).  Forward runs with these
+     * set also store, for every step it with 0 <= it-seg0 < nseg, at slot
+     * it-seg0 of [nseg][nshots][nx][pitch] buffers: the terms of the stress
+     * update that the new velocity v(it+1) enters through (D+ of it, masked
+     * as the stress update uses it) into seg_e[k] -- SH: exy, ezy; P-SV: exx,
+     * ezz, exz+ezx; spin: exx, ezz, exz+ezx, -vy_c - (ezx-exz)/2, Dx+ vy_c,
+     * Dz+ vy_c -- and the stress divergence including the sources of step it
+     * into seg_ds[c] (component slots as obs).  NULL skips. */
+    float *seg_e[6];
     float *seg_ds[3];
     int seg0, nseg;
+    /* Spin gradients of fwi_run_transposed (FP64 [nx][pitch], NULL skips):
+     * dL/dnu, dL/d(mu_c+nu_c), dL/d(dt/j). */
+    double *k_nu, *k_mnc, *k_buoj;
 } fwi_batch;
 
 /* ABI version of the loaded library (FWI_ABI_VERSION). */
@@ -190,7 +194,7 @@ long long fwi_multi_workspace_bytes(int n);
 int fwi_multi_prepare(fwi_batch *const *batches, int n, void *workspace);
 int fwi_multi_run(fwi_batch *const *batches, int n, void *workspace, int it0, int nsteps, void *stream);
 
-/* Exact discrete adjoint of fwi_run's SH / P-SV forward step, run backwards
+/* Exact discrete adjoint of fwi_run's SH / P-SV / spin forward step, run backwards
  * over forward steps it = it_hi-1 down to it_hi-nsteps on the adjoint state
  * held in the batch's stress and velocity buffers (sig~, v~; cleared by the
  * caller before the last step; disp is not used).  The adjoint displacement
@@ -199,8 +203,9 @@ int fwi_multi_run(fwi_batch *const *batches, int n, void *workspace, int it0, in
  * for entry e (fwi_trace_suffix_sum of the trace gradients; rows as for
  * fwi_run's injection, typically one per receiver and shot) and enters v~ as
  * dt * u~ at inj_cell[e].  Each step also accumulates, over every shot, into
- * the FP64 arrays: dL/dlam (k_lam, P-SV), dL/dmu (k_mu), dL/dbuo with buo =
- * dt/rho (k_rho); NULL skips an array.  Needs the forward strain of v(it+1)
+ * the FP64 arrays: dL/dlam (k_lam, P-SV and spin), dL/dmu (k_mu), dL/dbuo
+ * with buo = dt/rho (k_rho), and for spin k_nu, k_mnc, k_buoj; NULL skips an
+ * array.  Needs the forward strain of v(it+1)
  * and divergence of step it in seg_e / seg_ds for every step of the range
  * (written by a forward fwi_run over the same segment).  No counterpart in
  * the reference, whose adjoint (solver.py:290-329) is the continuous-adjoint
@@ -231,6 +236,11 @@ int fwi_misfit_tracegrad(const float *data, const float *syn, float *grad, doubl
  * Turns trace gradients (fwi_misfit_tracegrad) into the injection values of
  * fwi_run_transposed. */
 int fwi_trace_suffix_sum(const float *g, float *out, long long ntraces, int nt, void *stream);
+
+/* Source illumination for the learned preconditioner: acc[i] += sum over
+ * the nshots fields of f ([nshots][field]) of f^2, accumulated in FP64 in
+ * shot order.  No counterpart in the reference. */
+int fwi_energy_accumulate(const float *f, int nshots, long long field, double *acc, void *stream);
 
 /* Optimizer vector kernels (float32 vectors of n elements, FP64 arithmetic).
  * fwi_dot: *out = sum x[i]*y[i] in FP64, deterministic; partial is caller

@@ -13,7 +13,7 @@ from . import build as _build
 
 FWI_SH, FWI_PSV, FWI_SPIN = 0, 1, 2
 MODES = {"sh": FWI_SH, "psv": FWI_PSV, "spin": FWI_SPIN}
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 _fp = ctypes.POINTER(ctypes.c_float)
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -33,7 +33,8 @@ class FwiBatch(ctypes.Structure):
         ("nrec", ctypes.c_int), ("rec_cell", _vp), ("obs", _vp * 3),
         ("sae", ctypes.c_int), ("nsa", ctypes.c_int), ("snap_u", _vp * 3), ("snap_v", _vp * 3),
         ("k_lam", _vp), ("k_mu", _vp), ("k_rho", _vp),
-        ("seg_e", _vp * 3), ("seg_ds", _vp * 3), ("seg0", ctypes.c_int), ("nseg", ctypes.c_int),
+        ("seg_e", _vp * 6), ("seg_ds", _vp * 3), ("seg0", ctypes.c_int), ("nseg", ctypes.c_int),
+        ("k_nu", _vp), ("k_mnc", _vp), ("k_buoj", _vp),
     ]
 
 
@@ -85,6 +86,7 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
         "fwi_misfit_tracegrad": ([_vp, _vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                   _vp], ctypes.c_int),
         "fwi_trace_suffix_sum": ([_vp, _vp, ctypes.c_longlong, ctypes.c_int, _vp], ctypes.c_int),
+        "fwi_energy_accumulate": ([_vp, ctypes.c_int, ctypes.c_longlong, _vp, _vp], ctypes.c_int),
         "fwi_dot": ([_vp, _vp, ctypes.c_longlong, _vp, _vp, _vp], ctypes.c_int),
         "fwi_absmax": ([_vp, ctypes.c_longlong, _vp, _vp, _vp], ctypes.c_int),
         "fwi_axpby": ([_vp, ctypes.c_double, _vp, ctypes.c_double, _vp, ctypes.c_longlong, _vp], ctypes.c_int),

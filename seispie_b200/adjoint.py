@@ -23,13 +23,14 @@ import numpy as np
 import torch
 
 from . import engine
-from ._lib import FWI_PSV, FWI_SH
+from ._lib import FWI_PSV, FWI_SH, FWI_SPIN
 from .engine import COMP, NS, NV, DeviceModel, Grid, ShotBatch, adjoint_injection_lists, injection_lists
 
 
 def strain_fields(mode: int) -> int:
-    """Strain fields stored per step for the gradient (SH exy, ezy; P-SV exx, ezz, exz+ezx)."""
-    return 2 if mode == FWI_SH else 3
+    """Stress-update terms stored per step for the gradient (SH exy, ezy;
+    P-SV exx, ezz, exz+ezx; spin adds -vy_c - (ezx-exz)/2, Dx+ vy_c, Dz+ vy_c)."""
+    return 2 if mode == FWI_SH else 3 if mode == FWI_PSV else 6
 
 
 def default_segment(nt: int, mode: int, nshots: int, grid: Grid, budget_bytes: float | None = None) -> int:
@@ -45,18 +46,46 @@ def default_segment(nt: int, mode: int, nshots: int, grid: Grid, budget_bytes: f
     return min(k, nt)
 
 
+def two_level_segments(nt: int, mode: int) -> tuple:
+    """(K1, K2) minimising the memory of two-level checkpointing,
+    nt/K1 + K1/K2 checkpoints of S = NS+2NV fields plus K2 steps of
+    P = NE+NV stored fields: K2 = (S/P)^(2/3) nt^(1/3), K1 = sqrt(nt K2)."""
+    S = NS[mode] + 2 * NV[mode]
+    P = strain_fields(mode) + NV[mode]
+    k2 = max(1, int(round((S / P) ** (2.0 / 3.0) * nt ** (1.0 / 3.0))))
+    k1 = max(k2, int(round(math.sqrt(nt * k2))))
+    return min(k1, nt), min(k2, nt)
+
+
 class ExactAdjoint:
-    """Forward with checkpoints, then exact backward, for one batch of shots."""
+    """Forward with checkpoints, then exact backward, for one batch of shots.
+
+    levels = 1: a checkpoint every K steps; the backward recomputes each
+    segment once with the per-step stores (one extra forward sweep).
+    levels = 2: checkpoints every K1 = `segment` steps; the backward
+    recomputes a segment once to lay sub-checkpoints every K2 =
+    `sub_segment` steps inside it, then each sub-segment with the per-step
+    stores (two extra forward sweeps, memory nt/K1 + K1/K2 checkpoints and K2
+    steps of stores instead of nt/K checkpoints and K steps) -- recursive
+    checkpointing in the manner of revolve, two levels deep.  Both give the
+    same gradient bit for bit."""
 
     def __init__(self, model: DeviceModel, nt: int, src_id, isrc_of_shot, nshots: int, stf, rec_id,
-                 segment: int | None = None, tile: int = 0):
-        if model.mode not in (FWI_SH, FWI_PSV):
-            raise ValueError("the exact adjoint covers SH and P-SV")
+                 segment: int | None = None, tile: int = 0, levels: int = 1, sub_segment: int | None = None):
         self.model, self.nt, self.nshots = model, int(nt), int(nshots)
         self.rec_id = np.asarray(rec_id, np.int32)
         self.mode = model.mode
         g = model.grid
-        self.K = segment or default_segment(self.nt, self.mode, self.nshots, g)
+        if levels not in (1, 2):
+            raise ValueError("levels must be 1 or 2")
+        self.levels = levels
+        if levels == 1:
+            self.K = segment or default_segment(self.nt, self.mode, self.nshots, g)
+            self.K2 = self.K
+        else:
+            k1, k2 = two_level_segments(self.nt, self.mode)
+            self.K = segment or k1
+            self.K2 = min(sub_segment or k2, self.K)
         self.nseg = math.ceil(self.nt / self.K)
         self.fwd = ShotBatch(model, self.nshots, self.nt, self.rec_id, tile=tile)
         self.fdesc = self.fwd.desc(inj=injection_lists(self.nshots, src_id, isrc_of_shot), stf=stf)
@@ -64,21 +93,30 @@ class ExactAdjoint:
         shape = (self.nshots, g.nx, g.pitch)
         nstate = len(self.fwd.state_tensors())
         self.ckpt = torch.empty((self.nseg, nstate) + shape, dtype=torch.float32, device=dev)
-        self.seg_e = [None, None, None]
+        self.ckpt2 = (torch.empty((math.ceil(self.K / self.K2), nstate) + shape, dtype=torch.float32, device=dev)
+                      if levels == 2 else None)
+        self.seg_e = [None] * 6
         self.seg_ds = [None, None, None]
         for k in range(strain_fields(self.mode)):
-            self.seg_e[k] = torch.empty((self.K,) + shape, dtype=torch.float32, device=dev)
+            self.seg_e[k] = torch.empty((self.K2,) + shape, dtype=torch.float32, device=dev)
         for c in COMP[self.mode][: NV[self.mode]]:
-            self.seg_ds[c] = torch.empty((self.K,) + shape, dtype=torch.float32, device=dev)
+            self.seg_ds[c] = torch.empty((self.K2,) + shape, dtype=torch.float32, device=dev)
 
     def forward(self) -> list:
         """Run the forward, keeping a checkpoint every K steps; returns the
-        traces per component slot (None where absent), [nshots, nrec, nt]."""
+        traces per component slot (None where absent), [nshots, nrec, nt].
+        Also sums, over every checkpoint and shot, the squared particle
+        velocity into self.illum (FP64 [nx, pitch]): the source illumination
+        the learned preconditioner reads."""
         b = self.fwd
         b.clear()
+        g = self.model.grid
+        self.illum = torch.zeros((g.nx, g.pitch), dtype=torch.float64, device=self.model.device)
         for s in range(self.nseg):
             for q, t in enumerate(b.state_tensors()):
                 self.ckpt[s, q].copy_(t)
+            for v in b.vel[b.cur]:
+                engine.energy_accumulate(v, self.illum)
             n = min(self.K, self.nt - s * self.K)
             b.run(self.fdesc, False, s * self.K, n)
         return [b.traces(c).clone() if b.obs[c] is not None else None for c in range(3)]
@@ -86,10 +124,15 @@ class ExactAdjoint:
     def backward(self, g_traces: list) -> tuple:
         """Exact gradients from trace gradients (per component slot, each
         [nshots, nrec, nt] in forward time order).  Returns FP64
-        (dL/dlam, dL/dmu, dL/dbuo) on [nx, pitch] (dL/dlam is zero for SH)."""
+        (dL/dlam, dL/dmu, dL/dbuo) on [nx, pitch] (dL/dlam is zero for SH);
+        spin adds (dL/dnu, dL/dmnc, dL/dbuo_j) with mnc = mu_c + nu_c and
+        buo_j = dt/j.  Spin losses may depend on ux and uz only."""
+        if self.mode == FWI_SPIN and g_traces[1] is not None:
+            raise ValueError("the spin adjoint injects x and z trace gradients only (no uy_c term)")
         gr = self.model.grid
         dev = self.model.device
-        k = [torch.zeros((gr.nx, gr.pitch), dtype=torch.float64, device=dev) for _ in range(3)]
+        k = [torch.zeros((gr.nx, gr.pitch), dtype=torch.float64, device=dev)
+             for _ in range(6 if self.mode == FWI_SPIN else 3)]
         stf = [None, None, None]
         for c in range(3):
             if g_traces[c] is not None and self.fwd.obs[c] is not None:
@@ -101,15 +144,34 @@ class ExactAdjoint:
         inj = adjoint_injection_lists(self.nshots, self.rec_id) if len(self.rec_id) else None
         adesc = adj.desc(inj=inj, stf=stf, record=False, kernels=k)
         fwd = self.fwd
+
+        def reverse(t0, n):
+            """Recompute steps [t0, t0+n) from the current state with the
+            per-step stores and run their transposes."""
+            fwd.set_segment(self.fdesc, self.seg_e, self.seg_ds, t0, n)
+            fwd.run(self.fdesc, False, t0, n)
+            adj.set_segment(adesc, self.seg_e, self.seg_ds, t0, n)
+            adj.run_transposed(adesc, t0 + n, n)
+
         for s in reversed(range(self.nseg)):
             s0, n = s * self.K, min(self.K, self.nt - s * self.K)
             for q, t in enumerate(fwd.state_tensors()):
                 t.copy_(self.ckpt[s, q])
-            fwd.set_segment(self.fdesc, self.seg_e, self.seg_ds, s0, n)
-            fwd.run(self.fdesc, False, s0, n)
-            adj.set_segment(adesc, self.seg_e, self.seg_ds, s0, n)
-            adj.run_transposed(adesc, s0 + n, n)
-        fwd.set_segment(self.fdesc, [None] * 3, [None] * 3, 0, 0)
+            if self.levels == 1:
+                reverse(s0, n)
+                continue
+            nsub = math.ceil(n / self.K2)
+            fwd.set_segment(self.fdesc, [None] * 6, [None] * 3, 0, 0)
+            for jj in range(nsub):  # sub-checkpoints of this segment
+                for q, t in enumerate(fwd.state_tensors()):
+                    self.ckpt2[jj, q].copy_(t)
+                if jj < nsub - 1:
+                    fwd.run(self.fdesc, False, s0 + jj * self.K2, self.K2)
+            for jj in reversed(range(nsub)):
+                for q, t in enumerate(fwd.state_tensors()):
+                    t.copy_(self.ckpt2[jj, q])
+                reverse(s0 + jj * self.K2, min(self.K2, n - jj * self.K2))
+        fwd.set_segment(self.fdesc, [None] * 6, [None] * 3, 0, 0)
         return tuple(k)
 
 

@@ -277,6 +277,24 @@ __global__ void suffix_sum_kernel(const float *g, float *out, int nt) {
     }
 }
 
+// acc[i] += sum over shots s of f[s*field + i]^2 (FP64), shots in order.
+__global__ void energy_kernel(const float *f, int nshots, long long field, double *acc) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < field; i += (long long)gridDim.x * blockDim.x) {
+        double s = acc[i];
+        for (int k = 0; k < nshots; k++) {
+            const double v = f[k * field + i];
+            s += v * v;
+        }
+        acc[i] = s;
+    }
+}
+
+int launch_energy(const float *f, int nshots, long long field, double *acc, cudaStream_t st) {
+    long long b = (field + 255) / 256;
+    energy_kernel<<<(unsigned)(b > 4736 ? 4736 : b < 1 ? 1 : b), 256, 0, st>>>(f, nshots, field, acc);
+    return check_launch("energy");
+}
+
 int launch_suffix_sum(const float *g, float *out, long long ntraces, int nt, cudaStream_t st) {
     suffix_sum_kernel<<<(unsigned)ntraces, 256, 0, st>>>(g, out, nt);
     return check_launch("suffix_sum");

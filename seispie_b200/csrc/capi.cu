@@ -43,6 +43,7 @@ int launch_misfit(const float *data, const float *syn, float *adstf, double *mis
                   int nrec, int nt, double dt, cudaStream_t st, bool grad);
 long long misfit_partials(int nrec, int nt);
 int launch_suffix_sum(const float *g, float *out, long long ntraces, int nt, cudaStream_t st);
+int launch_energy(const float *f, int nshots, long long field, double *acc, cudaStream_t st);
 int launch_smooth(const double *in, int in_pitch, float *out, int out_pitch, double *tmp, int nx, int nz, int sigma,
                   cudaStream_t st);
 int launch_vps2lm(float *lam, float *mu, const float *rho, long long n, cudaStream_t st);
@@ -227,15 +228,17 @@ int fwi_run(fwi_batch *b, int adjoint, int it0, int nsteps, void *stream) {
 int fwi_run_transposed(fwi_batch *b, int it_hi, int nsteps, void *stream) {
     int rc = check_batch(b, 0, 0, 0);
     if (rc) return rc;
-    REQUIRE(b->mode == FWI_SH || b->mode == FWI_PSV, "fwi_run_transposed: SH or P-SV only");
+    REQUIRE(b->mode == FWI_SH || b->mode == FWI_PSV || b->mode == FWI_SPIN, "fwi_run_transposed: unknown mode");
     REQUIRE(nsteps >= 0 && it_hi - nsteps >= 0 && it_hi <= b->nt, "fwi_run_transposed: steps [%d, %d) outside [0, %d)",
             it_hi - nsteps, it_hi, b->nt);
     REQUIRE(it_hi - nsteps >= b->seg0 && it_hi <= b->seg0 + b->nseg,
             "fwi_run_transposed: steps [%d, %d) not stored in the segment [%d, %d)", it_hi - nsteps, it_hi, b->seg0,
             b->seg0 + b->nseg);
     const int cx = b->mode == FWI_SH ? 1 : 0;
-    REQUIRE(b->seg_e[0] && b->seg_e[1] && b->seg_ds[cx] && (b->mode == FWI_SH || (b->seg_e[2] && b->seg_ds[2])),
-            "fwi_run_transposed: the segment stores seg_e / seg_ds are required");
+    const int ne = b->mode == FWI_SH ? 2 : b->mode == FWI_PSV ? 3 : 6;
+    bool stores = b->seg_ds[cx] && (b->mode == FWI_SH || b->seg_ds[2]) && (b->mode != FWI_SPIN || b->seg_ds[1]);
+    for (int k = 0; k < ne; k++) stores = stores && b->seg_e[k];
+    REQUIRE(stores, "fwi_run_transposed: the segment stores seg_e / seg_ds are required");
     REQUIRE(b->k_mu, "fwi_run_transposed: k_mu is required");
     if (b->inj_ptr) {
         REQUIRE(b->inj_cell && b->inj_row, "inj_cell and inj_row are required with inj_ptr");
@@ -287,6 +290,13 @@ int fwi_trace_suffix_sum(const float *g, float *out, long long ntraces, int nt, 
     REQUIRE(ntraces >= 0 && ntraces <= 0x7fffffffll && nt >= 0, "fwi_trace_suffix_sum: ntraces in [0, 2^31), nt >= 0");
     if (ntraces == 0 || nt == 0) return 0;
     return launch_suffix_sum(g, out, ntraces, nt, (cudaStream_t)stream);
+}
+
+int fwi_energy_accumulate(const float *f, int nshots, long long field, double *acc, void *stream) {
+    REQUIRE(f && acc, "fwi_energy_accumulate: NULL pointer");
+    REQUIRE(nshots >= 0 && field >= 0, "fwi_energy_accumulate: negative size");
+    if (!nshots || !field) return 0;
+    return launch_energy(f, nshots, field, acc, (cudaStream_t)stream);
 }
 
 int fwi_smooth(const double *in, int in_pitch, float *out, int out_pitch, double *tmp, int nx, int nz, int sigma,

@@ -89,8 +89,9 @@ struct StepArgs {
     float *obs[3];
     float *snap_u[3];  // already offset to the slot, or NULL
     float *snap_v[3];
-    float *seg_e[3];   // per-step store of the strain of the new velocity (exact adjoint): SH exy, ezy |
-                       // P-SV exx, ezz, exz+ezx; slot-offset, or NULL
+    float *seg_e[6];   // per-step store of the stress-update terms of the new velocity (exact adjoint):
+                       // SH exy, ezy | P-SV exx, ezz, exz+ezx | spin also -vyc-(ezx-exz)/2, Dx+vyc,
+                       // Dz+vyc; slot-offset, or NULL
     float *seg_ds[3];  // per-step store of the stress divergence incl. sources, or NULL
 };
 
@@ -406,9 +407,18 @@ __device__ __forceinline__ void stress_update(const StepArgs &a, const float *s0
         }
         if (MODE == FWI_SPIN) {
             const float nu = ip[2 * FI], mnc = ip[3 * FI];
-            a.sig_out[4][g] = s0[4 * FS] + a.dt2 * nu * (-vyc - 0.5f * (vzx - vxz));
-            a.sig_out[3][g] = s0[3 * FS] + dt * mnc * dxp(2);
-            a.sig_out[5][g] = s0[5 * FS] + dt * mnc * dzp(2);
+            const float rot = -vyc - 0.5f * (vzx - vxz), eyx = dxp(2), eyz = dzp(2);
+            a.sig_out[4][g] = s0[4 * FS] + a.dt2 * nu * rot;
+            a.sig_out[3][g] = s0[3 * FS] + dt * mnc * eyx;
+            a.sig_out[5][g] = s0[5 * FS] + dt * mnc * eyz;
+            if (a.seg_e[0]) {
+                a.seg_e[0][g] = vxx;
+                a.seg_e[1][g] = vzz;
+                a.seg_e[2][g] = shear;
+                a.seg_e[3][g] = rot;
+                a.seg_e[4][g] = eyx;
+                a.seg_e[5][g] = eyz;
+            }
         }
     }
 }
@@ -904,13 +914,13 @@ int launch_step(const fwi_batch *b, int adjoint, int it, bool snap_u_next, int s
                                                                           : nullptr;
         a.snap_v[q] = (on && !adjoint && snap_v && b->snap_v[slot]) ? b->snap_v[slot] + snap_v_slot * field
                                                                      : nullptr;
-        const bool seg = on && !adjoint && b->mode != FWI_SPIN && it - b->seg0 >= 0 && it - b->seg0 < b->nseg;
+        const bool seg = on && !adjoint && it - b->seg0 >= 0 && it - b->seg0 < b->nseg;
         a.seg_ds[q] = (seg && b->seg_ds[slot]) ? b->seg_ds[slot] + (long long)(it - b->seg0) * field : nullptr;
     }
     {
-        const bool seg = !adjoint && b->mode != FWI_SPIN && it - b->seg0 >= 0 && it - b->seg0 < b->nseg;
-        const int ne = b->mode == FWI_SH ? 2 : 3;
-        for (int k = 0; k < 3; k++)
+        const bool seg = !adjoint && it - b->seg0 >= 0 && it - b->seg0 < b->nseg;
+        const int ne = b->mode == FWI_SH ? 2 : b->mode == FWI_PSV ? 3 : 6;
+        for (int k = 0; k < 6; k++)
             a.seg_e[k] = (seg && k < ne && b->seg_e[k]) ? b->seg_e[k] + (long long)(it - b->seg0) * field : nullptr;
     }
     if (b->mode == FWI_SH) {
@@ -947,8 +957,9 @@ static void forward_args(const fwi_batch *b, int cur, StepArgs &a) {
         a.vel_out[q] = on ? b->vel[nxt][q] : nullptr;
         a.disp[q] = on ? b->disp[q] : nullptr;
         a.obs[q] = on ? b->obs[comp_slot(b->mode, q)] : nullptr;
-        a.snap_u[q] = a.snap_v[q] = a.seg_e[q] = a.seg_ds[q] = nullptr;
+        a.snap_u[q] = a.snap_v[q] = a.seg_ds[q] = nullptr;
     }
+    for (int k = 0; k < 6; k++) a.seg_e[k] = nullptr;
     if (b->mode == FWI_SH) {
         a.stf[0] = b->stf[1];
         a.stf[1] = nullptr;
@@ -1117,22 +1128,23 @@ int multi_run(fwi_batch *const *bs, int n, void *ws, int it0, int nsteps, cudaSt
 struct AdjArgs {
     int nx, nz, pitch, nt, it, nshots;
     FastDiv divnz;
-    float cx1, cx2, cz1, cz2, dt;
-    float *sig_out[3];
-    float *vel_out[2];
-    const float *dsf[2];  // forward divergence of step it, per velocity component
-    const float *ef[3];   // forward strain of v(it+1): SH exy, ezy | P-SV exx, ezz, exz+ezx
-    double *k[3];         // SH: dL/dmu, dL/dbuo | P-SV: dL/dlam, dL/dmu, dL/dbuo ([nx][pitch], NULL skips)
+    float cx1, cx2, cz1, cz2, dt, dt2;
+    float *sig_out[6];
+    float *vel_out[3];
+    const float *dsf[3];  // forward divergence of step it, per velocity component
+    const float *ef[6];   // forward stress-update terms of v(it+1) (fwi_batch.seg_e)
+    double *k[6];         // SH: dL/dmu, dL/dbuo | P-SV: dL/dlam, dL/dmu, dL/dbuo |
+                          // spin: dL/dlam, dL/dmu, dL/dnu, dL/dmnc, dL/dbuo, dL/dbuo_j ([nx][pitch], NULL skips)
     const int *inj_ptr, *inj_cell, *inj_row;
     const float *g[2];    // u~ at the receivers per step (forward time order)
 };
 
 struct AdjMaps {
-    CUtensorMap sig[3];  // sig~, stress region box
-    CUtensorMap vel[2];  // v~, velocity region box
-    CUtensorMap ef[3];   // forward strain, interior box
-    CUtensorMap lm[2];   // SH: mu | P-SV: lam, mu; stress region box
-    CUtensorMap vp[2];   // dt/rho, sponge; velocity region box
+    CUtensorMap sig[6];  // sig~, stress region box
+    CUtensorMap vel[3];  // v~, velocity region box
+    CUtensorMap ef[6];   // forward stress-update terms, interior box
+    CUtensorMap lm[4];   // SH: mu | P-SV: lam, mu | spin: lam, mu, nu, mnc; stress region box
+    CUtensorMap vp[3];   // dt/rho, sponge (spin: dt/j); velocity region box
 };
 
 template <int MODE>
@@ -1141,21 +1153,23 @@ struct AdjTile {
     static constexpr int TX = 32, TZ = 32;
     static constexpr int SX = TX + 6, SZ = TZ + 8, VX = TX + 3, RVZ = TZ + 3;
     static constexpr int FS = (SX * SZ + 31) / 32 * 32, FV = (VX * SZ + 31) / 32 * 32;
-    static constexpr int NL = MODE == FWI_SH ? 1 : 2;  // stiffness fields
-    static constexpr int NK = MODE == FWI_SH ? 2 : 3;  // gradient fields
-    static constexpr int NE = MODE == FWI_SH ? 2 : 3;  // forward strain fields
+    static constexpr int NL = MODE == FWI_SH ? 1 : MODE == FWI_PSV ? 2 : 4;  // stiffness fields
+    static constexpr int NK = MODE == FWI_SH ? 2 : MODE == FWI_PSV ? 3 : 6;  // gradient fields
+    static constexpr int NE = MODE == FWI_SH ? 2 : MODE == FWI_PSV ? 3 : 6;  // forward stress-update terms
+    static constexpr int NP = MODE == FWI_SPIN ? 3 : 2;                      // velocity-region model fields
+    static constexpr int KB = MODE == FWI_SH ? 1 : MODE == FWI_PSV ? 2 : 4;  // gradient slot of dt/rho
     // sig~ (turned into t in place), v~, the forward strain of the interior,
     // the model tile, the injection list and three mbarriers (model, sig~,
     // v~ with strain)
     static constexpr int V_OFF = F::NS * FS, E_OFF = V_OFF + F::NV * FV;
     static constexpr int L_OFF = E_OFF + NE * TX * TZ, P_OFF = L_OFF + NL * FS;
-    static constexpr int LIST_OFF = P_OFF + 2 * FV;
+    static constexpr int LIST_OFF = P_OFF + NP * FV;
     static constexpr int LIST = kThreads * (1 + F::NINJ) + 8;
     static constexpr int BAR_OFF = (LIST_OFF + LIST + 1) / 2 * 2;
     static constexpr size_t bytes = sizeof(float) * (size_t)(BAR_OFF + 8);
     static constexpr uint32_t sig_bytes = 4u * F::NS * SX * SZ;
     static constexpr uint32_t vel_bytes = 4u * (F::NV * VX * SZ + NE * TX * TZ);
-    static constexpr uint32_t model_bytes = 4u * (NL * SX * SZ + 2 * VX * SZ);
+    static constexpr uint32_t model_bytes = 4u * (NL * SX * SZ + NP * VX * SZ);
     static_assert(NK * TX * TZ <= L_OFF, "gradient terms overlay the per-shot buffers");
     static_assert(vel_bytes < (1u << 20) && model_bytes < (1u << 20), "mbarrier transaction count limit");
 };
@@ -1212,8 +1226,29 @@ __device__ __forceinline__ void adj_apply(float *sV, int n, const int *sLoc, con
     }
 }
 
+// The velocity-like terms of the transposed step, (C^T t) per component,
+// from the transposed D+ of t (dxpT, dzpT) and, for spin, t4 at the cell:
+//   SH    a_y = Dx+^T t0 + Dz+^T t1
+//   P-SV  a_x = Dx+^T t0 + Dz+^T t2,  a_z = Dx+^T t2 + Dz+^T t1
+//   spin  a_x += Dz+^T t4 / 2,  a_z -= Dx+^T t4 / 2,  a_yc = -t4 + Dx+^T t3 + Dz+^T t5
+// (the transpose of stress_update's syy_c term dt2 nu (-vyc - (vzx - vxz)/2)).
+template <int MODE, class DXP, class DZP>
+__device__ __forceinline__ void adj_vel_terms(DXP dxpT, DZP dzpT, float t4c, float (&acc)[3]) {
+    if (MODE == FWI_SH) {
+        acc[0] = dxpT(0) + dzpT(1);
+    } else {
+        acc[0] = dxpT(0) + dzpT(2);
+        acc[1] = dxpT(2) + dzpT(1);
+        if (MODE == FWI_SPIN) {
+            acc[0] += 0.5f * dzpT(4);
+            acc[1] -= 0.5f * dxpT(4);
+            acc[2] = (dxpT(3) + dzpT(5)) - t4c;
+        }
+    }
+}
+
 template <int MODE>
-__global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : 3)
+__global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : MODE == FWI_PSV ? 3 : 1)
     adjoint_kernel(const __grid_constant__ AdjArgs a, const __grid_constant__ AdjMaps m) {
     using T = AdjTile<MODE>;
     using F = Fields<MODE>;
@@ -1272,7 +1307,7 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : 3)
 #pragma unroll
         for (int f = 0; f < NL; f++) tma_load_2d(sL + f * FS, &m.lm[f], z0 - 4, x0 - 3, &bar[0]);
 #pragma unroll
-        for (int p = 0; p < 2; p++) tma_load_2d(sP + p * FV, &m.vp[p], z0 - 4, x0 - 1, &bar[0]);
+        for (int p = 0; p < T::NP; p++) tma_load_2d(sP + p * FV, &m.vp[p], z0 - 4, x0 - 1, &bar[0]);
         if (crank < nshots) {
             issue_sig(crank);
             issue_vel(crank);
@@ -1347,6 +1382,18 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : 3)
                 s4[0] = xx;
                 s4[F4] = zz;
                 s4[2 * F4] = xz;
+                if (MODE == FWI_SPIN) {
+                    // t3 = dt mnc syx~, t4 = 2dt nu syy~, t5 = dt mnc syz~
+                    const float4 nu = l4[2 * F4], mn = l4[3 * F4];
+                    float4 a3 = s4[3 * F4], a4 = s4[4 * F4], a5 = s4[5 * F4];
+                    const float d2 = a.dt2;
+                    a3.x = dt * (mn.x * a3.x); a3.y = dt * (mn.y * a3.y); a3.z = dt * (mn.z * a3.z); a3.w = dt * (mn.w * a3.w);
+                    a5.x = dt * (mn.x * a5.x); a5.y = dt * (mn.y * a5.y); a5.z = dt * (mn.z * a5.z); a5.w = dt * (mn.w * a5.w);
+                    a4.x = d2 * (nu.x * a4.x); a4.y = d2 * (nu.y * a4.y); a4.z = d2 * (nu.z * a4.z); a4.w = d2 * (nu.w * a4.w);
+                    s4[3 * F4] = a3;
+                    s4[4 * F4] = a4;
+                    s4[5 * F4] = a5;
+                }
             }
         }
         // v~ and the forward strain of this shot; u~ enters v~ (thread 0)
@@ -1402,24 +1449,24 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : 3)
                     else
                         return cz1 * (t[-1] - t[0]) - cz2 * (t[-2] - t[1]);
                 };
-                float acc[2];
-                if (MODE == FWI_SH) {
-                    acc[0] = dxpT(0) + dzpT(1);
-                } else {
-                    acc[0] = dxpT(0) + dzpT(2);
-                    acc[1] = dxpT(2) + dzpT(1);
-                }
+                float acc[3];
+                adj_vel_terms<MODE>(dxpT, dzpT, MODE == FWI_SPIN ? trow[4 * FS] : 0.f, acc);
                 const float buo = sP[vi], bnd = sP[FV + vi];
                 const long long g = soff + (long long)gx * pitch + gz;
                 float gb = 0.f;
 #pragma unroll
                 for (int c = 0; c < NV; c++) {
                     const float vn = bnd * (sV[c * FV + vi] + acc[c]);
-                    sV[c * FV + vi] = buo * vn;
                     a.vel_out[c][g] = vn;
-                    gb += vn * dsv[c][q];
+                    if (MODE == FWI_SPIN && c == 2) {
+                        sV[c * FV + vi] = sP[2 * FV + vi] * vn;
+                        gk[T::KB + 1][q] += vn * dsv[c][q];
+                    } else {
+                        sV[c * FV + vi] = buo * vn;
+                        gb += vn * dsv[c][q];
+                    }
                 }
-                gk[NK - 1][q] += gb;
+                gk[T::KB][q] += gb;
             }
         };
         if (zedge) vel_interior(std::true_type{});
@@ -1457,16 +1504,14 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : 3)
                     const float *t = sS + f * FS + si;
                     return cz1 * (t[-1] * mzp(hz - 1) - t[0] * mzp(hz)) - cz2 * (t[-2] * mzp(hz - 2) - t[1] * mzp(hz + 1));
                 };
-                float acc[2];
-                if (MODE == FWI_SH) {
-                    acc[0] = dxpT(0) + dzpT(1);
-                } else {
-                    acc[0] = dxpT(0) + dzpT(2);
-                    acc[1] = dxpT(2) + dzpT(1);
-                }
-                const float buo = sP[vi], bnd = sP[FV + vi];
+                float acc[3];
+                adj_vel_terms<MODE>(dxpT, dzpT, MODE == FWI_SPIN ? sS[4 * FS + si] : 0.f, acc);
+                const float bnd = sP[FV + vi];
 #pragma unroll
-                for (int q = 0; q < NV; q++) sV[q * FV + vi] = buo * (bnd * (sV[q * FV + vi] + acc[q]));
+                for (int q = 0; q < NV; q++) {
+                    const float b = (MODE == FWI_SPIN && q == 2) ? sP[2 * FV + vi] : sP[vi];
+                    sV[q * FV + vi] = b * (bnd * (sV[q * FV + vi] + acc[q]));
+                }
             }
         }
         __syncthreads();
@@ -1516,6 +1561,15 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : 3)
                     const float exx = e[0], ezz = e[TX * TZ];
                     gk[0][q] += dt * ((sxx + szz) * (exx + ezz));
                     gk[1][q] += dt * (2.f * (sxx * exx + szz * ezz) + sxz * e[2 * TX * TZ]);
+                    if (MODE == FWI_SPIN) {
+                        // (A^T w): syx~ += (Dx-)^T w_y, syy~ += (Dz-)^T w_x - (Dx-)^T w_z + 2 w_y,
+                        // syz~ += (Dz-)^T w_y
+                        a.sig_out[3][g] = sg[3][q] + dxmT(2);
+                        a.sig_out[4][g] = sg[4][q] + ((dzmT(0) - dxmT(1)) + 2.f * vrow[2 * FV]);
+                        a.sig_out[5][g] = sg[5][q] + dzmT(2);
+                        gk[2][q] += a.dt2 * (sg[4][q] * e[3 * TX * TZ]);
+                        gk[3][q] += dt * (sg[3][q] * e[4 * TX * TZ] + sg[5][q] * e[5 * TX * TZ]);
+                    }
                 }
             }
         };
@@ -1557,10 +1611,10 @@ static int adjoint_maps(const fwi_batch *b, const AdjArgs &a, AdjMaps &m) {
     for (int f = 0; f < F::NS && !rc; f++) rc = encode_map(&m.sig[f], b->sig[cur][f], 3, pitch, nx, ns, T::SZ, T::SX);
     for (int q = 0; q < F::NV && !rc; q++) rc = encode_map(&m.vel[q], b->vel[cur][q], 3, pitch, nx, ns, T::SZ, T::VX);
     for (int k = 0; k < T::NE && !rc; k++) rc = encode_map(&m.ef[k], a.ef[k], 3, pitch, nx, ns, T::TZ, T::TX);
-    const float *lm[2] = {MODE == FWI_SH ? b->mu : b->lam, b->mu};
+    const float *lm[4] = {MODE == FWI_SH ? b->mu : b->lam, b->mu, b->nu, b->mnc};
     for (int f = 0; f < T::NL && !rc; f++) rc = encode_map(&m.lm[f], lm[f], 2, pitch, nx, 1, T::SZ, T::SX);
-    const float *vp[2] = {b->buo, b->bound};
-    for (int p = 0; p < 2 && !rc; p++) rc = encode_map(&m.vp[p], vp[p], 2, pitch, nx, 1, T::SZ, T::VX);
+    const float *vp[3] = {b->buo, b->bound, b->buo_j};
+    for (int p = 0; p < T::NP && !rc; p++) rc = encode_map(&m.vp[p], vp[p], 2, pitch, nx, 1, T::SZ, T::VX);
     return rc;
 }
 
@@ -1595,7 +1649,7 @@ static int launch_adjoint(const fwi_batch *b, const AdjArgs &a, cudaStream_t st)
     int rc = adjoint_maps<MODE>(b, a, m);
     if (rc) return rc;
     const int C = adjoint_cluster(b->nshots, (long long)((b->nz + T::TZ - 1) / T::TZ) * ((b->nx + T::TX - 1) / T::TX),
-                                  MODE == FWI_SH ? 4 : 3);
+                                  MODE == FWI_SH ? 4 : MODE == FWI_PSV ? 3 : 1);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((b->nz + T::TZ - 1) / T::TZ, (b->nx + T::TX - 1) / T::TX, C);
     cfg.blockDim = dim3(kThreads, 1, 1);
@@ -1629,30 +1683,42 @@ int launch_adjoint_step(const fwi_batch *b, int it, cudaStream_t st) {
     a.cz1 = (float)(9.0 / (8.0 * (double)b->dz));
     a.cz2 = (float)(1.0 / (24.0 * (double)b->dz));
     a.dt = (float)b->dt;
-    const bool sh = b->mode == FWI_SH;
-    const int nxt = 1 - b->cur, ns = sh ? 2 : 3, nv = sh ? 1 : 2, ne = sh ? 2 : 3;
-    for (int f = 0; f < 3; f++) a.sig_out[f] = f < ns ? b->sig[nxt][f] : nullptr;
-    for (int q = 0; q < 2; q++) a.vel_out[q] = q < nv ? b->vel[nxt][q] : nullptr;
+    a.dt2 = (float)(2.0 * b->dt);
+    const int mode = b->mode;
+    const int nxt = 1 - b->cur, ns = nfields_sig(mode), nv = nfields_vel(mode);
+    const int ne = mode == FWI_SH ? 2 : mode == FWI_PSV ? 3 : 6;
+    for (int f = 0; f < 6; f++) a.sig_out[f] = f < ns ? b->sig[nxt][f] : nullptr;
+    for (int q = 0; q < 3; q++) a.vel_out[q] = q < nv ? b->vel[nxt][q] : nullptr;
     const long long field = (long long)b->nshots * b->nx * b->pitch;
     const long long slot = it - b->seg0;
-    for (int k = 0; k < 3; k++) a.ef[k] = k < ne ? b->seg_e[k] + slot * field : nullptr;
-    a.dsf[0] = b->seg_ds[sh ? 1 : 0] + slot * field;
-    a.dsf[1] = sh ? nullptr : b->seg_ds[2] + slot * field;
-    if (sh) {
+    for (int k = 0; k < 6; k++) a.ef[k] = k < ne ? b->seg_e[k] + slot * field : nullptr;
+    for (int q = 0; q < 3; q++) a.dsf[q] = q < nv ? b->seg_ds[comp_slot(mode, q)] + slot * field : nullptr;
+    for (int k = 0; k < 6; k++) a.k[k] = nullptr;
+    if (mode == FWI_SH) {
         a.k[0] = b->k_mu;
         a.k[1] = b->k_rho;
-        a.k[2] = nullptr;
     } else {
         a.k[0] = b->k_lam;
         a.k[1] = b->k_mu;
-        a.k[2] = b->k_rho;
+        if (mode == FWI_PSV) {
+            a.k[2] = b->k_rho;
+        } else {
+            a.k[2] = b->k_nu;
+            a.k[3] = b->k_mnc;
+            a.k[4] = b->k_rho;
+            a.k[5] = b->k_buoj;
+        }
     }
     a.inj_ptr = b->inj_ptr;
     a.inj_cell = b->inj_cell;
     a.inj_row = b->inj_row;
-    a.g[0] = sh ? b->stf[1] : b->stf[0];
-    a.g[1] = sh ? nullptr : b->stf[2];
-    return sh ? launch_adjoint<FWI_SH>(b, a, st) : launch_adjoint<FWI_PSV>(b, a, st);
+    a.g[0] = mode == FWI_SH ? b->stf[1] : b->stf[0];
+    a.g[1] = mode == FWI_SH ? nullptr : b->stf[2];
+    switch (mode) {
+        case FWI_SH: return launch_adjoint<FWI_SH>(b, a, st);
+        case FWI_PSV: return launch_adjoint<FWI_PSV>(b, a, st);
+        default: return launch_adjoint<FWI_SPIN>(b, a, st);
+    }
 }
 
 }  // namespace fwi

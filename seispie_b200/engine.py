@@ -182,6 +182,7 @@ class ShotBatch:
 
     # ------------------------------------------------------------ descriptors
     def desc(self, inj=None, stf=(None, None, None), record=True, kernels=(None, None, None)) -> FwiBatch:
+        """kernels: FP64 accumulators (k_lam, k_mu, k_rho[, k_nu, k_mnc, k_buoj])."""
         g, m = self.grid, self.model
         b = FwiBatch()
         b.mode, b.nx, b.nz, b.pitch = self.mode, g.nx, g.nz, g.pitch
@@ -211,14 +212,16 @@ class ShotBatch:
             b.snap_u[c] = ptr(self.snap_u[c])
             b.snap_v[c] = ptr(self.snap_v[c])
         b.sae, b.nsa = self.sae, self.nsa
-        b.k_lam, b.k_mu, b.k_rho = (ptr(k) for k in kernels)
+        kernels = tuple(kernels) + (None,) * (6 - len(kernels))
+        b.k_lam, b.k_mu, b.k_rho, b.k_nu, b.k_mnc, b.k_buoj = (ptr(k) for k in kernels)
         return b
 
     def set_segment(self, b: FwiBatch, seg_e, seg_ds, seg0: int, nseg: int) -> FwiBatch:
         """Point a descriptor at per-step segment stores (exact adjoint):
         strain fields seg_e[k] and divergence per component slot seg_ds[c]."""
+        for k in range(6):
+            b.seg_e[k] = ptr(seg_e[k]) if k < len(seg_e) else None
         for c in range(3):
-            b.seg_e[c] = ptr(seg_e[c])
             b.seg_ds[c] = ptr(seg_ds[c])
         b.seg0, b.nseg = int(seg0), int(nseg)
         return b
@@ -338,6 +341,13 @@ def trace_suffix_sum(g: torch.Tensor, out: torch.Tensor | None = None, stream=No
     check(_lib.load().fwi_trace_suffix_sum(ptr(g), ptr(out), g.numel() // max(nt, 1), nt, stream_handle(stream)),
           "fwi_trace_suffix_sum")
     return out
+
+
+def energy_accumulate(f: torch.Tensor, acc: torch.Tensor, stream=None) -> None:
+    """acc += sum over the leading (shot) axis of f^2, FP64 (fwi_energy_accumulate)."""
+    field = acc.numel()
+    check(_lib.load().fwi_energy_accumulate(ptr(f), f.numel() // max(field, 1), field, ptr(acc), stream_handle(stream)),
+          "fwi_energy_accumulate")
 
 
 def smooth(k: torch.Tensor, grid: Grid, sigma: int, stream=None) -> torch.Tensor:

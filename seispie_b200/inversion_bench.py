@@ -26,12 +26,17 @@ import numpy as np
 
 
 def write_case(root: str, nx: int, nz: int, shots: int, nrec: int, nt: int, niter: int, sigma: int, sae: int,
-               h: float = 10.0, dt: float = 1e-3, square: int = 64, amp: float = 0.08):
+               h: float = 10.0, dt: float = 1e-3, square: int = 64, amp: float = 0.08, board=None,
+               method: str = "lbfgs", optimize_extra: str = ""):
+    """board: perturbation pattern in [-1, 1] ([nx, nz]; default the
+    checkerboard of `square`-cell squares); method / optimize_extra: the
+    [optimize] method and further keys (lines) of the inversion config."""
     from .io import write_model
     i, j = np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij")
     vp0 = 3000.0 + 300.0 * (j / (nz - 1) - 0.5)
     vs0 = vp0 / np.sqrt(3.0)
-    board = np.where(((i // square) + (j // square)) % 2 == 0, 1.0, -1.0)
+    if board is None:
+        board = np.where(((i // square) + (j // square)) % 2 == 0, 1.0, -1.0)
     rho = np.full(nx * nz, 2600.0)
     true = dict(vp=(vp0 * (1 + amp * board)).ravel(), vs=(vs0 * (1 + amp * board)).ravel(), rho=rho)
     init = dict(vp=vp0.ravel(), vs=vs0.ravel(), rho=rho)
@@ -55,9 +60,9 @@ def write_case(root: str, nx: int, nz: int, shots: int, nrec: int, nt: int, nite
                 % (sae, sigma))
     os.makedirs(os.path.join(root, "inverse"), exist_ok=True)
     with open(os.path.join(root, "inverse", "config.ini"), "w") as f:
-        f.write("[workflow]\nmode = inversion\ninherit = adjoint\n\n[optimize]\nniter = %d\nmethod = lbfgs\n"
-                "ls_step = 10\nls_step_max = 0.5\nls_step_init = 0.05\nls_thresh = 1.2\nlbfgs_mem = 5\n\n"
-                "[path]\noutput = output\n" % niter)
+        f.write("[workflow]\nmode = inversion\ninherit = adjoint\n\n[optimize]\nniter = %d\nmethod = %s\n"
+                "ls_step = 10\nls_step_max = 0.5\nls_step_init = 0.05\nls_thresh = 1.2\nlbfgs_mem = 5\n%s\n"
+                "[path]\noutput = output\n" % (niter, method, optimize_extra))
     return 2600.0 * true["vs"] ** 2
 
 

@@ -159,4 +159,6 @@ class sgd(base):
     """sgd.py:5-57 is a verbatim copy of base.run; kept as an alias."""
 
 
-__all__ = ["base", "cg", "gd", "lbfgs", "sgd", "bracket", "backtrack", "VecOps"]
+from .learned import lbfgs_learned  # noqa: E402  (needs lbfgs above)
+
+__all__ = ["base", "cg", "gd", "lbfgs", "lbfgs_learned", "sgd", "bracket", "backtrack", "VecOps"]

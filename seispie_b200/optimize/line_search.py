@@ -40,8 +40,13 @@ class bracket:
     def _trial(self, m_new, p_new, alpha):
         self.solver.update_model_device(self.ops.axpby(1.0, m_new, alpha, p_new))
 
-    def run(self, m_new, g_new, p_new, f) -> int:
-        """bracket.py:32-81."""
+    def run(self, m_new, g_new, p_new, f, allow_restart: bool = True) -> int:
+        """bracket.py:32-81.  allow_restart = False returns the failure status
+        instead of restarting the search along the same direction (used when
+        a caller has another direction to fall back to).  The reference
+        restarts by recursing without limit; a restarted search repeats the
+        same trial steps, so a second failure is returned instead of
+        recursing until the interpreter's stack is exhausted."""
         if self.head:
             print("  step 1")
         ops = self.ops
@@ -71,12 +76,12 @@ class bracket:
             if status < 0:
                 self.solver.update_model_device(m_new)
                 neg_g = ops.axpby(-1.0, g_new)
-                if self.angle(p_new, neg_g) < 1e-3:
+                if self.angle(p_new, neg_g) < 1e-3 or not allow_restart:
                     return status
                 if self.head:
                     print("  restarting line search")
                 self.restart()
-                return self.run(m_new, g_new, p_new, f)
+                return self.run(m_new, g_new, p_new, f, allow_restart=False)
 
     def get_history(self, i):
         """bracket.py:83-89."""

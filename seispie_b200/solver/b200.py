@@ -243,12 +243,15 @@ class b200:
         return b
 
     def _exact(self, mode) -> bool:
-        """Gradient by the exact discrete adjoint?  Default: yes for P-SV (the
-        reference's P-SV adjoint cannot run, solver.py:324-329), no for SH
-        (its continuous-adjoint kernel equals dt times the exact gradient)."""
+        """Gradient by the exact discrete adjoint?  Default: yes for P-SV and
+        spin (the reference's adjoint cannot run for them, solver.py:324-329),
+        no for SH (its continuous-adjoint kernel equals dt times the exact
+        gradient).  Spin has no continuous-adjoint kernel here."""
         g = self.config.get("gradient", "")
+        if mode == FWI_SPIN:
+            return True
         if g in ("exact", "reference"):
-            return g == "exact" and mode in (FWI_SH, FWI_PSV)
+            return g == "exact"
         return mode == FWI_PSV
 
     def _exact_gradient(self, mode, shots, data_of) -> float:
@@ -265,6 +268,7 @@ class b200:
                 ea = ExactAdjoint(self.model, nt, self.src_id, lambda s: -1 if combine else chunk[s], n,
                                   self._stf(mode), self.rec_id, tile=self.tile)
                 tr = ea.forward()
+                self.illum_f64 += ea.illum
                 grads = [None, None, None]
                 for c, lst in data_of:
                     data = torch.from_numpy(np.stack([lst[shots.index(i)] for i in chunk]))
@@ -273,12 +277,20 @@ class b200:
                     syn = tr[c].reshape(-1).contiguous()
                     misfit += float(engine.misfit_tracegrad(data, syn, grads[c], n, nrec, nt, self.dt).sum().item())
                     grads[c] = grads[c].view(n, nrec, nt)
-                k_lam, k_mu, k_buo = ea.backward(grads)
+                ks = ea.backward(grads)
+                k_lam, k_mu, k_buo = ks[:3]
                 self.k_lam_f64 += self.dt * k_lam
                 self.k_mu_f64 += self.dt * k_mu
                 # buo = dt/rho: dchi/drho = -dchi/dbuo * dt / rho^2
                 rho = self.model.rho.double()
                 self.k_rho_f64 -= self.dt * k_buo * self.dt / torch.where(rho > 0, rho * rho, torch.ones_like(rho))
+                if mode == FWI_SPIN:
+                    # spin: nu, mu_c and nu_c (both through mnc = mu_c + nu_c), j through dt/j
+                    k_nu, k_mnc, k_buoj = ks[3:]
+                    jj = self.model.j.double()
+                    self.k_nu_f64 += self.dt * k_nu
+                    self.k_mnc_f64 += self.dt * k_mnc
+                    self.k_j_f64 -= self.dt * k_buoj * self.dt / torch.where(jj > 0, jj * jj, torch.ones_like(jj))
                 del ea
         return misfit
 
@@ -422,11 +434,30 @@ class b200:
             self.k_lam_f64 = torch.zeros((g.nx, g.pitch), dtype=torch.float64, device=self.device)
             self.k_mu_f64 = torch.zeros((g.nx, g.pitch), dtype=torch.float64, device=self.device)
             self.k_rho_f64 = torch.zeros((g.nx, g.pitch), dtype=torch.float64, device=self.device)
+            self.illum_f64 = torch.zeros((g.nx, g.pitch), dtype=torch.float64, device=self.device)
+            # spin gradients (dt * dchi/dnu, dt * dchi/d(mu_c) = dt * dchi/d(nu_c), dt * dchi/dj)
+            self.k_nu_f64 = torch.zeros((g.nx, g.pitch), dtype=torch.float64, device=self.device)
+            self.k_mnc_f64 = torch.zeros((g.nx, g.pitch), dtype=torch.float64, device=self.device)
+            self.k_j_f64 = torch.zeros((g.nx, g.pitch), dtype=torch.float64, device=self.device)
 
     def clear_kernels(self):
         with self._ctx():
-            for k in (self.k_lam_f64, self.k_mu_f64, self.k_rho_f64):
+            for k in (self.k_lam_f64, self.k_mu_f64, self.k_rho_f64, self.illum_f64, self.k_nu_f64, self.k_mnc_f64,
+                      self.k_j_f64):
                 k.zero_()
+
+    def illumination_device(self):
+        """Source illumination of the last exact-adjoint gradient (squared
+        particle velocity summed over checkpoints and shots), float32 CUDA
+        vector of npt, or None when the gradient did not come from the exact
+        adjoint.  No counterpart in the reference; read by the learned
+        preconditioner."""
+        if not getattr(self, "_illum_valid", False):
+            return None
+        with self._ctx():
+            out = self.illum_f64[:, : self.nz].float().reshape(-1).clone()
+        self.stream.synchronize()
+        return out
 
     def run_adjoint(self):
         """solver.py:290-329 for the batch of the last run_kernel chunk."""
@@ -440,6 +471,7 @@ class b200:
             print("Computing kernels" if adj else "Computing misfit")
         self.setup_adjoint()
         self.clear_kernels()
+        self._illum_valid = bool(adj) and all(self._exact(m) for m in self.modes)
         shots = self._shots()
         misfit = 0.0
         data_of = {FWI_SH: [(1, self.syn_y)], FWI_PSV: [(0, self.syn_x), (2, self.syn_z)],
@@ -494,14 +526,18 @@ class b200:
         solver.py:380-393, which also counted the local kernel twice)."""
         if hasattr(self.mpi, "allreduce_tensor"):
             self.stream.synchronize()
-            for k in (self.k_lam_f64, self.k_mu_f64, self.k_rho_f64):
+            for k in self._summed_fields():
                 self.mpi.allreduce_tensor(k)
         else:
-            for k in (self.k_lam_f64, self.k_mu_f64, self.k_rho_f64):
+            for k in self._summed_fields():
                 host = k.cpu().numpy()
                 out = np.zeros_like(host)
                 self.mpi.sum(host, out)
                 k.copy_(torch.from_numpy(out))
+
+    def _summed_fields(self):
+        return (self.k_lam_f64, self.k_mu_f64, self.k_rho_f64, self.illum_f64, self.k_nu_f64, self.k_mnc_f64,
+                self.k_j_f64)
 
     def compute_misfit(self):
         return self.run_kernel(0)

@@ -239,3 +239,49 @@ class UNet:
         check(self.lib.fwi_unet_mse(ptr(out), ptr(target), ptr(gout), ptr(loss), ptr(part), out.numel(),
                                     stream_handle(None)), "fwi_unet_mse")
         return loss, gout
+
+
+def bench(h: int = 2048, w: int = 1024, reps: int = 20) -> list:
+    """TFLOP/s of the 3x3 convolution (forward, data and weight gradients) at
+    the four U-Net levels of an h x w image (CUDA events, after warm-up)."""
+    from .engine import check, ptr, stream_handle
+    lib = _lib.load()
+    dev = torch.device("cuda")
+    st = stream_handle(None)
+    out = []
+    for lvl, c in enumerate(CH):
+        hh, ww = h >> lvl, w >> lvl
+        x = torch.randn(1, hh, ww, c, device=dev).to(torch.bfloat16)
+        wt = (torch.randn(9 * c * c, device=dev) * 0.05).to(torch.bfloat16)
+        wd = torch.empty_like(wt)
+        y = torch.empty_like(x)
+        b = torch.zeros(c, device=dev)
+        part = torch.empty(lib.fwi_unet_wgrad_partials(c, c, 1, hh, ww), device=dev)
+        dw = torch.empty(9 * c * c, device=dev)
+        flops = 2.0 * hh * ww * 9 * c * c
+        res = dict(level=lvl, image=[hh, ww], channels=c)
+        for name, fn in (
+                ("fwd", lambda: lib.fwi_unet_conv3x3(ptr(x), c, None, 0, ptr(wt), ptr(b), c, ptr(y), c, None, 0, 1, hh,
+                                                     ww, 1, st)),
+                ("dgrad", lambda: lib.fwi_unet_conv3x3(ptr(x), c, None, 0, ptr(wd), None, c, ptr(y), c, None, 0, 1,
+                                                       hh, ww, 0, st)),
+                ("wgrad", lambda: lib.fwi_unet_conv3x3_wgrad(ptr(x), c, ptr(y), c, None, 0, 1, hh, ww, ptr(part),
+                                                             ptr(dw), None, st))):
+            for _ in range(3):
+                check(fn(), name)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            res[name + "_us"] = ms * 1e3
+            res[name + "_tflops"] = flops / (ms * 1e-3) / 1e12
+        out.append(res)
+    return out
+
+
+if __name__ == "__main__":
+    import json
+    print(json.dumps(bench()))

@@ -269,3 +269,105 @@ def test_exact_gradient_many_shots_tiles_receivers(mode):
     for k in grad:
         scale = np.abs(grad[k]).max()
         np.testing.assert_allclose(grad[k], total[k], rtol=0, atol=2e-5 * scale, err_msg=k)
+
+
+def test_spin_exact_gradient_directional_derivatives():
+    """Micropolar spin: the exact adjoint's gradient along a smooth direction
+    of each of the seven parameters (rho, lam, mu, nu, j, mu_c, nu_c) against
+    central finite differences of the FP64 oracle's misfit (x and z traces)."""
+    from seispie_b200 import engine
+    from seispie_b200.adjoint import AcquisitionSetup, ExactAdjoint, hann_taper
+    from seispie_b200.engine import Grid, build_model
+    nx, nz, nt, h, dt = 40, 36, 240, 10.0, 1e-3
+    i, j = np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij")
+    sm = lambda a, b, c: np.sin(a * i / nx + b * j / nz + c)  # noqa: E731
+    p = dict(rho=2700 * (1 + 0.03 * sm(1.7, 2.9, 2.0)), lam=8.1e9 * (1 + 0.05 * sm(3.1, 2.2, 0.3)),
+             mu=8.1e9 * (1 + 0.04 * sm(2.3, 3.7, 1.1)), nu=1.005e9 * (1 + 0.05 * sm(1.3, 2.1, 0.7)),
+             j=2700 * (1 + 0.05 * sm(2.9, 1.1, 0.2)), mu_c=1.5e8 * (1 + 0.05 * sm(1.9, 2.7, 1.4)),
+             nu_c=3.0e8 * (1 + 0.05 * sm(0.9, 3.3, 2.5)))
+    p = {k: v.astype(np.float32) for k, v in p.items()}
+    src = np.array([[120.0, 150.0, 0, 14.0, 0.07, 25.0, 1e10], [260.0, 90.0, 0, 12.0, 0.08, -40.0, 1e10]])
+    rec = np.array([[50.0 + 45 * r, 30.0 + 40 * (r % 3)] for r in range(6)])
+    absorb = (8, 0.05, 1, 1, 1, 0)
+    grid = Grid(nx, nz, h, h)
+    setup = AcquisitionSetup("spin", grid, dt, nt, src, rec, absorb, segment=37)
+    o = Oracle("f64")
+    stf = source_time_functions(src, nt, dt)
+    w = hann_taper(nt, dt) ** 2
+    bound = o.set_bound(nx, nz, *absorb)
+    nrec = len(setup.rec_id)
+
+    def traces(q):
+        out = []
+        for s in range(setup.nshots):
+            prm = dict(bound=bound, **{k: np.asarray(v, np.float64).ravel() for k, v in q.items()})
+            obs, _, _ = o.forward("spin", nx, nz, h, h, dt, nt, prm, setup.src_id, stf, s, setup.rec_id)
+            out.append([obs[c].reshape(-1, nt) for c in "xz"])
+        return np.array(out)  # [shot, component, receiver, t]
+
+    q = {k: v.astype(np.float64) for k, v in p.items()}
+    q["mu"] = q["mu"] * (1 + 0.03 * np.cos(np.arange(nx * nz).reshape(nx, nz) * 0.37))
+    data = traces(q)
+
+    def chi(q):
+        r = traces(q) - data
+        return float((w * r * r).sum())
+
+    m = build_model("spin", grid, dt, {k: v.ravel() for k, v in p.items()}, absorb, "cuda")
+    ea = ExactAdjoint(m, nt, setup.src_id, setup.isrc_of_shot, setup.nshots, setup.stf, setup.rec_id, segment=37)
+    tr = ea.forward()
+    g = [None, None, None]
+    for ci, c in enumerate((0, 2)):
+        d = torch.as_tensor(np.ascontiguousarray(data[:, ci]).astype(np.float32), device="cuda").reshape(-1)
+        g[c] = torch.empty(setup.nshots * nrec * nt, device="cuda")
+        engine.misfit_tracegrad(d, tr[c].reshape(-1).contiguous(), g[c], setup.nshots, nrec, nt, dt)
+        g[c] = g[c].view(setup.nshots, nrec, nt)
+    k = ea.backward(g)
+    dlam, dmu, dbuo, dnu, dmnc, dbuoj = (t[:, :nz].double().cpu().numpy() for t in k)
+    grad = dict(lam=dlam, mu=dmu, nu=dnu, mu_c=dmnc, nu_c=dmnc,
+                rho=-dbuo * dt / p["rho"].astype(np.float64) ** 2, j=-dbuoj * dt / p["j"].astype(np.float64) ** 2)
+    eps = 1e-5
+    for n, name in enumerate(("rho", "lam", "mu", "nu", "j", "mu_c", "nu_c")):
+        direction = (0.5 + 0.5 * np.sin(0.21 * i + 0.13 * j + n)) * p[name].astype(np.float64)
+        qp = {kk: v.astype(np.float64) for kk, v in p.items()}
+        qm = {kk: v.astype(np.float64) for kk, v in p.items()}
+        qp[name] = qp[name] + eps * direction
+        qm[name] = qm[name] - eps * direction
+        fd = (chi(qp) - chi(qm)) / (2 * eps)
+        dd = float((grad[name] * direction).sum())
+        assert abs(dd - fd) < 2e-3 * abs(fd), (name, dd, fd)
+
+
+@pytest.mark.parametrize("mode", ["psv", "spin"])
+def test_two_level_checkpointing_is_bit_identical(mode):
+    """Recursive (two-level) checkpointing recomputes the same forward steps,
+    so its gradient equals the single-level one exactly."""
+    from seispie_b200.adjoint import AcquisitionSetup, ExactAdjoint
+    from seispie_b200.engine import Grid, build_model
+    nx, nz, nt, h, dt = 40, 36, 230, 10.0, 1e-3
+    rng = np.random.default_rng(6)
+    src = np.array([[120.0, 150.0, 0, 14.0, 0.07, 25.0, 1e10], [260.0, 90.0, 0, 12.0, 0.08, -40.0, 1e10]])
+    rec = np.array([[50.0 + 45 * r, 30.0 + 40 * (r % 3)] for r in range(6)])
+    absorb = (8, 0.05, 1, 1, 1, 0)
+    grid = Grid(nx, nz, h, h)
+    setup = AcquisitionSetup(mode, grid, dt, nt, src, rec, absorb)
+    npt = nx * nz
+    prm = dict(rho=np.full(npt, 2700.0), lam=np.full(npt, 8.1e9) * (1 + 0.05 * rng.random(npt)),
+               mu=np.full(npt, 8.1e9) * (1 + 0.05 * rng.random(npt)))
+    if mode == "spin":
+        prm.update(nu=np.full(npt, 1.005e9), j=np.full(npt, 2700.0), mu_c=np.full(npt, 1.5e8), nu_c=np.full(npt, 3e8))
+    m = build_model(mode, grid, dt, prm, absorb, "cuda")
+    nrec = len(setup.rec_id)
+    g = [torch.randn(setup.nshots, nrec, nt, device="cuda") if c != 1 else None for c in range(3)]
+    out = []
+    for kw in (dict(segment=37), dict(levels=2, segment=50, sub_segment=7)):
+        ea = ExactAdjoint(m, nt, setup.src_id, setup.isrc_of_shot, setup.nshots, setup.stf, setup.rec_id, **kw)
+        tr = ea.forward()
+        out.append((tr, ea.backward(g)))
+    (tr1, k1), (tr2, k2) = out
+    for c in (0, 2):
+        assert torch.equal(tr1[c], tr2[c])
+    assert len(k1) == (6 if mode == "spin" else 3)
+    for a, b in zip(k1, k2):
+        assert torch.equal(a, b)
+    assert float(k1[1].abs().max()) > 0
