@@ -2,7 +2,7 @@
 
     python -m seispie_b200.learned gen   --out DIR [--cases 60 --nx 256 --nz 128 --shots 16 --nt 1500 --niter 10]
     python -m seispie_b200.learned train --data DIR --weights W.npz [--epochs 30]
-    python -m seispie_b200.learned eval  --weights W.npz [--nx 512 --nz 256 --shots 32 --nt 2500 --niter 12]
+    python -m seispie_b200.learned eval  [--weights W.npz --nx 512 --nz 256 --shots 32 --nt 2500 --niter 12]
 
 gen runs plain L-BFGS inversions (the reference's step logic, exact P-SV
 gradient, mu as the model variable as in the reference's workflow) on random
@@ -32,6 +32,11 @@ import numpy as np
 import torch
 
 from .unet import UNet
+
+
+# weights trained by ``gen`` + ``train`` with their defaults (1494 pairs of
+# 256 x 128 P-SV mu inversions, 30 epochs)
+DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "unet_psv_mu.npz")
 
 
 def _pad8(n: int) -> int:
@@ -235,7 +240,7 @@ def main(argv=None):
     t.add_argument("--lr", type=float, default=1e-3)
     t.add_argument("--seed", type=int, default=0)
     e = sub.add_parser("eval")
-    e.add_argument("--weights", required=True)
+    e.add_argument("--weights", default=DEFAULT_WEIGHTS)
     e.add_argument("--nx", type=int, default=512)
     e.add_argument("--nz", type=int, default=256)
     e.add_argument("--shots", type=int, default=32)

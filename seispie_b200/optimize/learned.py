@@ -3,13 +3,15 @@
 The step logic is the reference's L-BFGS (optimize/lbfgs.py:5-59) with its
 backtracking line search; on top of it:
 
-* ``unet_weights = <file.npz>``: at every iteration the U-Net
-  (seispie_b200.unet) maps (gradient, source illumination, model) to an
-  update direction, scaled to the max-norm of the L-BFGS direction.  It is
-  used only if it is a descent direction (g.p < 0) and its line search
-  succeeds; otherwise the plain L-BFGS direction is searched from a clean
-  line-search history.  The L-BFGS memory is built from model and gradient
-  differences either way.
+* ``unet_weights = <file.npz>``: in the first ``learned_iterations``
+  iterations (default ``lbfgs_mem``: while the L-BFGS memory is still
+  short) the U-Net (seispie_b200.unet) maps (gradient, source illumination,
+  model) to an update direction, scaled to the max-norm of the L-BFGS
+  direction.  It is used only if it is a descent direction (g.p < 0) and its
+  line search succeeds; otherwise the plain L-BFGS direction is searched
+  from a clean line-search history.  The L-BFGS memory is built from model
+  and gradient differences either way, so the later L-BFGS iterations start
+  from the learned steps' curvature pairs.
 * ``record_pairs = <file.npz>``: stores, per iteration, the gradient, the
   illumination, the model and the accepted update m_{k+1} - m_k -- the
   training pairs of the preconditioner.
@@ -37,12 +39,16 @@ class lbfgs_learned(lbfgs):
         self.pairs = []
         self.learned_accepted = 0
         self.learned_rejected = 0
+        get = self.config.get if hasattr(self.config, "get") else (lambda k, d=None: d)
+        self.learned_iterations = int(get("learned_iterations", str(self.lbfgs_mem)))
+        self.iteration = 0
 
     def compute_direction(self):
         p_plain = super().compute_direction()
         self.p_plain, self.used_learned = p_plain, False
         self.illum = self.solver.illumination_device()
-        if self.pre is None or self.illum is None:
+        self.iteration += 1
+        if self.pre is None or self.illum is None or self.iteration > self.learned_iterations:
             return p_plain
         p = self.pre.direction(self.g_new, self.illum, self.m_new, self.solver.nx, self.solver.nz,
                                self.ops.absmax(p_plain))

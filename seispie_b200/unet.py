@@ -96,17 +96,20 @@ class UNet:
     def state(self) -> dict:
         return dict(w=self.w.cpu().numpy(), step=self.step)
 
-    def save(self, path: str) -> None:
-        np.savez(path, w=self.w.cpu().numpy(), m=self.m.cpu().numpy(), v=self.v.cpu().numpy(), step=self.step)
+    def save(self, path: str, optimizer_state: bool = True) -> None:
+        """Weights (and, unless optimizer_state is False, the Adam state)."""
+        extra = dict(m=self.m.cpu().numpy(), v=self.v.cpu().numpy(), step=self.step) if optimizer_state else {}
+        np.savez_compressed(path, w=self.w.cpu().numpy(), **extra)
 
     @classmethod
     def load(cls, path: str, device="cuda") -> "UNet":
         z = np.load(path)
         net = cls(device)
         net.load_flat(z["w"])
-        net.m.copy_(torch.as_tensor(z["m"]))
-        net.v.copy_(torch.as_tensor(z["v"]))
-        net.step = int(z["step"])
+        if "m" in z:
+            net.m.copy_(torch.as_tensor(z["m"]))
+            net.v.copy_(torch.as_tensor(z["v"]))
+            net.step = int(z["step"])
         return net
 
     # ----------------------------------------------------------- kernels
