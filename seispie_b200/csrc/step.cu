@@ -1180,15 +1180,17 @@ struct AdjTile {
 // list (block-wide; the count it returns is block-uniform) and may run
 // while the staging copies are in flight; adj_apply adds them once v~ has
 // landed and the list is visible to thread 0.
+// adj_fetch: this thread's entry base + tid (its shared-memory location in
+// the staged v~, or -1, and its u~ values); no barrier, so it can be issued
+// well before adj_compact needs it.
 template <int MODE>
-__device__ __forceinline__ int adj_collect(const AdjArgs &a, int base, int p1, int x0, int z0, int *sLoc,
-                                           float *sVal, int *sWarp) {
+__device__ __forceinline__ void adj_fetch(const AdjArgs &a, int base, int p1, int x0, int z0, int &loc,
+                                          float (&val)[Fields<MODE>::NINJ]) {
     using T = AdjTile<MODE>;
-    constexpr int NINJ = Fields<MODE>::NINJ;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int e = base + tid;
-    int loc = -1;
-    float val[NINJ];
+    const int e = base + (int)threadIdx.x;
+    loc = -1;
+#pragma unroll
+    for (int c = 0; c < Fields<MODE>::NINJ; c++) val[c] = 0.f;
     if (e < p1) {
         const int k = a.inj_cell[e];
         const int gx = fdiv(k, a.divnz), gz = k - gx * a.nz;
@@ -1197,9 +1199,16 @@ __device__ __forceinline__ int adj_collect(const AdjArgs &a, int base, int p1, i
             loc = rx * T::SZ + rz + 3;
             const long long src = (long long)a.inj_row[e] * a.nt + a.it;
 #pragma unroll
-            for (int c = 0; c < NINJ; c++) val[c] = a.g[c][src];
+            for (int c = 0; c < Fields<MODE>::NINJ; c++) val[c] = a.g[c][src];
         }
     }
+}
+
+template <int MODE>
+__device__ __forceinline__ int adj_compact(int loc, const float (&val)[Fields<MODE>::NINJ], int *sLoc, float *sVal,
+                                           int *sWarp) {
+    constexpr int NINJ = Fields<MODE>::NINJ;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned ball = __ballot_sync(0xffffffffu, loc >= 0);
     if (lane == 0) sWarp[warp] = __popc(ball);
     __syncthreads();
@@ -1214,6 +1223,15 @@ __device__ __forceinline__ int adj_collect(const AdjArgs &a, int base, int p1, i
         for (int c = 0; c < NINJ; c++) sVal[c * kThreads + pos] = val[c];
     }
     return n;
+}
+
+template <int MODE>
+__device__ __forceinline__ int adj_collect(const AdjArgs &a, int base, int p1, int x0, int z0, int *sLoc,
+                                           float *sVal, int *sWarp) {
+    int loc;
+    float val[Fields<MODE>::NINJ];
+    adj_fetch<MODE>(a, base, p1, x0, z0, loc, val);
+    return adj_compact<MODE>(loc, val, sLoc, sVal, sWarp);
 }
 
 template <int MODE>
@@ -1320,6 +1338,15 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : MODE == FWI_PSV
 #pragma unroll
         for (int q = 0; q < RPW; q++) gk[k][q] = 0.f;
 
+    // injection entries of the next shot, fetched a shot ahead (one entry
+    // per thread; shots with more entries than threads are collected later)
+    int nx_loc = -1;
+    float nx_val[F::NINJ];
+    auto prefetch_entries = [&](int shot) {
+        const int q0 = a.inj_ptr ? a.inj_ptr[shot] : 0, q1 = a.inj_ptr ? a.inj_ptr[shot + 1] : 0;
+        if (q1 - q0 <= kThreads) adj_fetch<MODE>(a, q0, q1, x0, z0, nx_loc, nx_val);
+    };
+    if (crank < nshots) prefetch_entries(crank);
     int i = 0;
     for (int shot = crank; shot < nshots; shot += csize, i++) {
         const long long soff = (long long)shot * nx * pitch;
@@ -1335,7 +1362,7 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : MODE == FWI_PSV
         const int p0 = a.inj_ptr ? a.inj_ptr[shot] : 0, p1 = a.inj_ptr ? a.inj_ptr[shot + 1] : 0;
         const bool single = p1 - p0 <= kThreads;
         int n_in = 0;
-        if (single && p1 > p0) n_in = adj_collect<MODE>(a, p0, p1, x0, z0, sLoc, sVal, sWarp);
+        if (single && p1 > p0) n_in = adj_compact<MODE>(nx_loc, nx_val, sLoc, sVal, sWarp);
 
         // sig~ of the interior cells into registers (t overwrites it)
         bool ok = mbar_wait(&bar[1], i & 1);
@@ -1517,6 +1544,7 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : MODE == FWI_PSV
         __syncthreads();
         // t has been consumed: the next shot's sig~ streams in during the stress half
         if (tid == 0 && shot + csize < nshots) issue_sig(shot + csize);
+        if (shot + csize < nshots) prefetch_entries(shot + csize);
 
         // ---- sig~' and the stiffness gradient terms on the interior; b v~'
         // rows x-1 .. x+2 in a register window, pre-masked
