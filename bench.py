@@ -8,9 +8,12 @@ spaced at z = 10 cells, 256 receivers at z = 12 cells, dt = 1e-3 s,
 nt = 4000, 20-cell sponge on the left, right and bottom, adjoint interval 10,
 smoothing sigma 4.  Observed data come from the checkerboard model (computed
 once, untimed).  One step = one gradient of all 32 shots: batched forward with
-snapshots, misfit and adjoint source, batched adjoint with the k_lam/k_mu
-interaction, Gaussian smoothing.  Cell-updates per step =
-32 * 512 * 512 * 4000 * 2 (forward and adjoint counted separately).
+checkpoints, misfit and trace gradients, exact discrete adjoint (checkpointed
+recomputation + transposed steps with the lambda / mu / rho terms), Gaussian
+smoothing (``--gradient reference``: forward with snapshots and the
+snapshot-correlation adjoint instead).  Cell-updates per step =
+32 * 512 * 512 * 4000 * 2 (forward and adjoint counted separately; recomputed
+forward steps are not counted).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -91,7 +94,7 @@ def config_of(a, w, extra=None):
     c = {"workload": "psv_gradient_%dx%d_shots%d_rec%d_nt%d" % (a.nx, a.nz, a.shots, a.nrec, a.nt),
          "grid": [a.nx, a.nz], "shots": a.shots, "receivers": a.nrec, "nt": a.nt, "adjoint_interval": a.sae,
          "smooth_sigma": a.sigma, "cells_per_step": 2 * a.shots * a.nx * a.nz * a.nt,
-         "l2": "inputs larger than L2 (wavefields of all shots and the snapshots exceed 126 MB); no flush",
+         "l2": "inputs larger than L2 (each wavefield field of the 32 shots is 32 MiB, the state 7 fields, the checkpoints 23 GiB: far above the 126 MB L2); no flush",
          "parallelism": "shots", "gradient": a.gradient}
     if extra:
         c.update(extra)

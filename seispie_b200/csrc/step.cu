@@ -1150,7 +1150,8 @@ struct AdjMaps {
 template <int MODE>
 struct AdjTile {
     using F = Fields<MODE>;
-    static constexpr int TX = 32, TZ = 32;
+    // spin holds twice the fields: 16 x 32 tiles keep two CTAs per SM
+    static constexpr int TX = MODE == FWI_SPIN ? 16 : 32, TZ = 32;
     static constexpr int SX = TX + 6, SZ = TZ + 8, VX = TX + 3, RVZ = TZ + 3;
     static constexpr int FS = (SX * SZ + 31) / 32 * 32, FV = (VX * SZ + 31) / 32 * 32;
     static constexpr int NL = MODE == FWI_SH ? 1 : MODE == FWI_PSV ? 2 : 4;  // stiffness fields
@@ -1266,7 +1267,7 @@ __device__ __forceinline__ void adj_vel_terms(DXP dxpT, DZP dzpT, float t4c, flo
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : MODE == FWI_PSV ? 3 : 1)
+__global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : MODE == FWI_PSV ? 3 : 2)
     adjoint_kernel(const __grid_constant__ AdjArgs a, const __grid_constant__ AdjMaps m) {
     using T = AdjTile<MODE>;
     using F = Fields<MODE>;
@@ -1677,7 +1678,7 @@ static int launch_adjoint(const fwi_batch *b, const AdjArgs &a, cudaStream_t st)
     int rc = adjoint_maps<MODE>(b, a, m);
     if (rc) return rc;
     const int C = adjoint_cluster(b->nshots, (long long)((b->nz + T::TZ - 1) / T::TZ) * ((b->nx + T::TX - 1) / T::TX),
-                                  MODE == FWI_SH ? 4 : MODE == FWI_PSV ? 3 : 1);
+                                  MODE == FWI_SH ? 4 : MODE == FWI_PSV ? 3 : 2);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((b->nz + T::TZ - 1) / T::TZ, (b->nx + T::TX - 1) / T::TX, C);
     cfg.blockDim = dim3(kThreads, 1, 1);

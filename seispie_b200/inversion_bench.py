@@ -27,10 +27,13 @@ import numpy as np
 
 def write_case(root: str, nx: int, nz: int, shots: int, nrec: int, nt: int, niter: int, sigma: int, sae: int,
                h: float = 10.0, dt: float = 1e-3, square: int = 64, amp: float = 0.08, board=None,
-               method: str = "lbfgs", optimize_extra: str = ""):
+               method: str = "lbfgs", optimize_extra: str = "", perturb: str = "both"):
     """board: perturbation pattern in [-1, 1] ([nx, nz]; default the
-    checkerboard of `square`-cell squares); method / optimize_extra: the
-    [optimize] method and further keys (lines) of the inversion config."""
+    checkerboard of `square`-cell squares); perturb: "both" (vp and vs), "vs"
+    (vs only) or "mu" (vs with vp adjusted so that lambda keeps its starting
+    value: the model error is then in the inverted parameter mu alone);
+    method / optimize_extra: the [optimize] method and further keys
+    (lines) of the inversion config."""
     from .io import write_model
     i, j = np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij")
     vp0 = 3000.0 + 300.0 * (j / (nz - 1) - 0.5)
@@ -38,7 +41,14 @@ def write_case(root: str, nx: int, nz: int, shots: int, nrec: int, nt: int, nite
     if board is None:
         board = np.where(((i // square) + (j // square)) % 2 == 0, 1.0, -1.0)
     rho = np.full(nx * nz, 2600.0)
-    true = dict(vp=(vp0 * (1 + amp * board)).ravel(), vs=(vs0 * (1 + amp * board)).ravel(), rho=rho)
+    vs_true = vs0 * (1 + amp * board)
+    if perturb == "both":
+        vp_true = vp0 * (1 + amp * board)
+    elif perturb == "mu":  # lambda of the background kept: only mu differs from the start
+        vp_true = np.sqrt(vp0 ** 2 - 2 * vs0 ** 2 + 2 * vs_true ** 2)
+    else:
+        vp_true = vp0
+    true = dict(vp=vp_true.ravel(), vs=vs_true.ravel(), rho=rho)
     init = dict(vp=vp0.ravel(), vs=vs0.ravel(), rho=rho)
     fwd = os.path.join(root, "forward")
     write_model(os.path.join(fwd, "model_true"), nx, nz, h, h, true)

@@ -91,12 +91,12 @@ def random_board(rng, nx: int, nz: int) -> np.ndarray:
 
 
 def run_inversion(root: str, nx: int, nz: int, shots: int, nt: int, niter: int, board, amp: float, method: str,
-                  extra: str = "", sigma: int = 4, nrec: int | None = None):
+                  extra: str = "", sigma: int = 4, nrec: int | None = None, perturb: str = "both"):
     """One inversion through the workflow; returns (optimizer, wall seconds)."""
     from . import workflow
     from .inversion_bench import write_case
     write_case(root, nx, nz, shots, nrec or max(16, nx // 4), nt, niter, sigma, 10, board=board, amp=amp,
-               method=method, optimize_extra=extra)
+               method=method, optimize_extra=extra, perturb=perturb)
     t0 = time.time()
     with contextlib.redirect_stdout(io.StringIO()):
         wf = workflow.main(["--workdir", os.path.join(root, "inverse")])
@@ -114,7 +114,7 @@ def cmd_gen(a):
         path = os.path.abspath(os.path.join(a.out, "pairs_%04d.npz" % c))
         with tempfile.TemporaryDirectory() as root:
             run_inversion(root, a.nx, a.nz, a.shots, a.nt, a.niter, board, amp, "lbfgs_learned",
-                          "record_pairs = %s\n" % path)
+                          "record_pairs = %s\n" % path, perturb=a.perturb)
         if os.path.exists(path):
             npairs += len(np.load(path)["g"])
         print(json.dumps({"case": c, "pairs": npairs, "seconds": time.time() - t0}), flush=True)
@@ -205,10 +205,12 @@ def cmd_eval(a):
     for label, method, extra in (("plain", "lbfgs", ""),
                                  ("learned", "lbfgs_learned", "unet_weights = %s\n" % os.path.abspath(a.weights))):
         with tempfile.TemporaryDirectory() as root:
-            opt, wall = run_inversion(root, a.nx, a.nz, a.shots, a.nt, a.niter, board, a.amp, method, extra)
+            opt, wall = run_inversion(root, a.nx, a.nz, a.shots, a.nt, a.niter, board, a.amp, method, extra,
+                                      perturb=a.perturb)
         res[label] = _summary(opt, wall)
         print(json.dumps({label: res[label]}), flush=True)
-    print(json.dumps({"workload": "psv_inversion_%dx%d_shots%d_nt%d_lbfgs%d" % (a.nx, a.nz, a.shots, a.nt, a.niter),
+    print(json.dumps({"workload": "psv_inversion_%dx%d_shots%d_nt%d_lbfgs%d_%s" % (a.nx, a.nz, a.shots, a.nt, a.niter,
+                                                                                  a.perturb),
                       "plain_final_ratio": res["plain"]["final_ratio"],
                       "learned_final_ratio": res["learned"]["final_ratio"],
                       "plain_time_to_90pct_drop_s": res["plain"]["time_to_90pct_drop_s"],
@@ -232,6 +234,7 @@ def main(argv=None):
     g.add_argument("--niter", type=int, default=10)
     g.add_argument("--seed", type=int, default=1)
     g.add_argument("--max-seconds", type=float, default=0, help="stop after this long (0: no limit)")
+    g.add_argument("--perturb", default="both", choices=["both", "vs", "mu"])
     t = sub.add_parser("train")
     t.add_argument("--data", required=True)
     t.add_argument("--weights", required=True)
@@ -249,6 +252,8 @@ def main(argv=None):
     e.add_argument("--amp", type=float, default=0.08)
     e.add_argument("--random-model", action="store_true", help="random board instead of the 64-cell checkerboard")
     e.add_argument("--seed", type=int, default=12345)
+    e.add_argument("--perturb", default="both", choices=["both", "vs", "mu"],
+                   help="mu: perturb only mu (lambda kept), so that the mu-only inversion can fit the data")
     a = ap.parse_args(argv)
     {"gen": cmd_gen, "train": cmd_train, "eval": cmd_eval}[a.cmd](a)
 
