@@ -267,7 +267,10 @@ def main():
     if a.gradient == "exact":
         # exact discrete adjoint with checkpointed recomputation (the P-SV gradient of the solver)
         from seispie_b200.adjoint import ExactAdjoint
-        ea = ExactAdjoint(m_init, nt, sid, lambda s: s, nshots, stf, rid, tile=a.tile)
+        # per-step stores of the last steps kept from the forward sweep in half of the free HBM
+        free, _ = torch.cuda.mem_get_info(dev)
+        ea = ExactAdjoint(m_init, nt, sid, lambda s: s, nshots, stf, rid, tile=a.tile, tail_memory=0.5 * free)
+        checkpointing = {"segment": ea.K, "checkpoints": ea.nseg, "stored_tail_steps": ea.tail}
         grads = [torch.empty((nshots, a.nrec, nt), dtype=torch.float32, device=dev) if c != 1 else None
                  for c in range(3)]
         b = ea.fwd
@@ -396,6 +399,8 @@ def main():
 
     if rank == 0:
         extra = {"tile": _lib.tile_label(b_tile(a, tuned)), "misfit": misfit_total}
+        if a.gradient == "exact":
+            extra["checkpointing"] = checkpointing
         if tuned:
             extra["autotune_ms_per_fwd_step"] = tuned[2]
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,

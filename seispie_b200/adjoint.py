@@ -68,10 +68,16 @@ class ExactAdjoint:
     stores (two extra forward sweeps, memory nt/K1 + K1/K2 checkpoints and K2
     steps of stores instead of nt/K checkpoints and K steps) -- recursive
     checkpointing in the manner of revolve, two levels deep.  Both give the
-    same gradient bit for bit."""
+    same gradient bit for bit.
+
+    tail_memory (bytes): HBM the forward sweep may fill with the per-step
+    stores of its last steps; those steps are then transposed without being
+    recomputed (exactly the same values, so the same gradient), and only the
+    steps before them are checkpointed."""
 
     def __init__(self, model: DeviceModel, nt: int, src_id, isrc_of_shot, nshots: int, stf, rec_id,
-                 segment: int | None = None, tile: int = 0, levels: int = 1, sub_segment: int | None = None):
+                 segment: int | None = None, tile: int = 0, levels: int = 1, sub_segment: int | None = None,
+                 tail_memory: float = 0.0):
         self.model, self.nt, self.nshots = model, int(nt), int(nshots)
         self.rec_id = np.asarray(rec_id, np.int32)
         self.mode = model.mode
@@ -86,7 +92,11 @@ class ExactAdjoint:
             k1, k2 = two_level_segments(self.nt, self.mode)
             self.K = segment or k1
             self.K2 = min(sub_segment or k2, self.K)
-        self.nseg = math.ceil(self.nt / self.K)
+        field = 4 * self.nshots * g.nx * g.pitch
+        per_step = (strain_fields(self.mode) + NV[self.mode]) * field
+        self.tail = min(self.nt, int(max(0.0, tail_memory) // per_step))
+        self.t0 = self.nt - self.tail  # steps [t0, nt) keep their stores from the forward sweep
+        self.nseg = math.ceil(self.t0 / self.K)
         self.fwd = ShotBatch(model, self.nshots, self.nt, self.rec_id, tile=tile)
         self.fdesc = self.fwd.desc(inj=injection_lists(self.nshots, src_id, isrc_of_shot), stf=stf)
         dev = model.device
@@ -101,6 +111,12 @@ class ExactAdjoint:
             self.seg_e[k] = torch.empty((self.K2,) + shape, dtype=torch.float32, device=dev)
         for c in COMP[self.mode][: NV[self.mode]]:
             self.seg_ds[c] = torch.empty((self.K2,) + shape, dtype=torch.float32, device=dev)
+        self.tail_e, self.tail_ds = [None] * 6, [None, None, None]
+        if self.tail:
+            for k in range(strain_fields(self.mode)):
+                self.tail_e[k] = torch.empty((self.tail,) + shape, dtype=torch.float32, device=dev)
+            for c in COMP[self.mode][: NV[self.mode]]:
+                self.tail_ds[c] = torch.empty((self.tail,) + shape, dtype=torch.float32, device=dev)
 
     def forward(self) -> list:
         """Run the forward, keeping a checkpoint every K steps; returns the
@@ -117,8 +133,15 @@ class ExactAdjoint:
                 self.ckpt[s, q].copy_(t)
             for v in b.vel[b.cur]:
                 engine.energy_accumulate(v, self.illum)
-            n = min(self.K, self.nt - s * self.K)
+            n = min(self.K, self.t0 - s * self.K)
             b.run(self.fdesc, False, s * self.K, n)
+        if self.tail:
+            b.set_segment(self.fdesc, self.tail_e, self.tail_ds, self.t0, self.tail)
+            for s0 in range(self.t0, self.nt, self.K):
+                for v in b.vel[b.cur]:
+                    engine.energy_accumulate(v, self.illum)
+                b.run(self.fdesc, False, s0, min(self.K, self.nt - s0))
+            b.set_segment(self.fdesc, [None] * 6, [None] * 3, 0, 0)
         return [b.traces(c).clone() if b.obs[c] is not None else None for c in range(3)]
 
     def backward(self, g_traces: list) -> tuple:
@@ -153,8 +176,11 @@ class ExactAdjoint:
             adj.set_segment(adesc, self.seg_e, self.seg_ds, t0, n)
             adj.run_transposed(adesc, t0 + n, n)
 
+        if self.tail:
+            adj.set_segment(adesc, self.tail_e, self.tail_ds, self.t0, self.tail)
+            adj.run_transposed(adesc, self.nt, self.tail)
         for s in reversed(range(self.nseg)):
-            s0, n = s * self.K, min(self.K, self.nt - s * self.K)
+            s0, n = s * self.K, min(self.K, self.t0 - s * self.K)
             for q, t in enumerate(fwd.state_tensors()):
                 t.copy_(self.ckpt[s, q])
             if self.levels == 1:

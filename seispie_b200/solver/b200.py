@@ -265,8 +265,13 @@ class b200:
         for chunk in self._chunks(shots, mode, True):
             n = len(chunk)
             with self._ctx():
+                # the last steps keep their per-step stores from the forward sweep in part of the free
+                # HBM (those steps are not recomputed; the gradient is the same); not when the
+                # configuration caps the memory of a batch
+                free, _ = torch.cuda.mem_get_info(self.device)
+                tail = 0.4 * free if self.batch_memory <= 0 else 0.0
                 ea = ExactAdjoint(self.model, nt, self.src_id, lambda s: -1 if combine else chunk[s], n,
-                                  self._stf(mode), self.rec_id, tile=self.tile)
+                                  self._stf(mode), self.rec_id, tile=self.tile, tail_memory=tail)
                 tr = ea.forward()
                 self.illum_f64 += ea.illum
                 grads = [None, None, None]

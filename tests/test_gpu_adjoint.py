@@ -340,8 +340,9 @@ def test_spin_exact_gradient_directional_derivatives():
 
 @pytest.mark.parametrize("mode", ["psv", "spin"])
 def test_two_level_checkpointing_is_bit_identical(mode):
-    """Recursive (two-level) checkpointing recomputes the same forward steps,
-    so its gradient equals the single-level one exactly."""
+    """Recursive (two-level) checkpointing, and per-step stores kept from the
+    forward sweep for the last steps, produce the same forward values as
+    single-level recomputation, so the gradients are equal exactly."""
     from seispie_b200.adjoint import AcquisitionSetup, ExactAdjoint
     from seispie_b200.engine import Grid, build_model
     nx, nz, nt, h, dt = 40, 36, 230, 10.0, 1e-3
@@ -359,15 +360,21 @@ def test_two_level_checkpointing_is_bit_identical(mode):
     m = build_model(mode, grid, dt, prm, absorb, "cuda")
     nrec = len(setup.rec_id)
     g = [torch.randn(setup.nshots, nrec, nt, device="cuda") if c != 1 else None for c in range(3)]
+    # per-step stores kept from the forward sweep for the last 61 steps
+    per_step = (6 + 3 if mode == "spin" else 3 + 2) * 4 * setup.nshots * nx * grid.pitch
     out = []
-    for kw in (dict(segment=37), dict(levels=2, segment=50, sub_segment=7)):
+    for kw in (dict(segment=37), dict(levels=2, segment=50, sub_segment=7),
+               dict(segment=37, tail_memory=61.5 * per_step)):
         ea = ExactAdjoint(m, nt, setup.src_id, setup.isrc_of_shot, setup.nshots, setup.stf, setup.rec_id, **kw)
         tr = ea.forward()
         out.append((tr, ea.backward(g)))
-    (tr1, k1), (tr2, k2) = out
-    for c in (0, 2):
-        assert torch.equal(tr1[c], tr2[c])
+        if "tail_memory" in kw:
+            assert ea.tail == 61 and ea.t0 == nt - 61
+    (tr1, k1) = out[0]
     assert len(k1) == (6 if mode == "spin" else 3)
-    for a, b in zip(k1, k2):
-        assert torch.equal(a, b)
+    for tr2, k2 in out[1:]:
+        for c in (0, 2):
+            assert torch.equal(tr1[c], tr2[c])
+        for a, b in zip(k1, k2):
+            assert torch.equal(a, b)
     assert float(k1[1].abs().max()) > 0
