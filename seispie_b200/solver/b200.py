@@ -22,7 +22,6 @@ Differences that a caller can see, all deliberate:
 """
 from __future__ import annotations
 
-import os
 from os import makedirs, path
 from time import time
 
@@ -30,7 +29,7 @@ import numpy as np
 import torch
 
 from .. import engine
-from .._lib import FWI_PSV, FWI_SH, FWI_SPIN, MODES
+from .._lib import FWI_PSV, FWI_SH, FWI_SPIN
 from ..engine import DeviceModel, Grid, ShotBatch
 
 

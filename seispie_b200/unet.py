@@ -13,7 +13,6 @@ input has 3 channels, packed into 16 for the tensor-core convolutions.
 """
 from __future__ import annotations
 
-import ctypes
 
 import numpy as np
 import torch

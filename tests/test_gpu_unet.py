@@ -6,7 +6,6 @@ agree to FP32 summation order (plus one bf16 rounding of stored
 activations); the whole network is compared with a torch model that rounds
 its activations to bf16 at the same points (straight-through in backward).
 """
-import numpy as np
 import pytest
 
 torch = pytest.importorskip("torch")
