@@ -8,9 +8,10 @@ gen runs plain L-BFGS inversions (the reference's step logic, exact P-SV
 gradient, mu as the model variable as in the reference's workflow) on random
 checkerboard and smooth-layer models and records, per iteration, the
 smoothed gradient, the source illumination, the model and the accepted
-update m_{k+1} - m_k.  train fits the BF16 U-Net (seispie_b200.unet) to map
-the first three to the direction of the fourth (each normalised, MSE loss,
-Adam).  eval runs the same inversion twice, plain and with
+update m_{k+1} - m_k (and the case's true mu).  train fits the BF16 U-Net
+(seispie_b200.unet) to map the first three to the direction of the fourth
+(each normalised, MSE loss, Adam); ``--target error`` trains on the model
+error m_true - m_k instead.  eval runs the same inversion twice, plain and with
 ``method = lbfgs_learned`` (the learned direction where it is a descent
 direction and passes the line search, L-BFGS otherwise), and prints both
 misfit histories with wall-clock times, the time to a 50 % and a 90 % misfit
@@ -92,15 +93,16 @@ def random_board(rng, nx: int, nz: int) -> np.ndarray:
 
 def run_inversion(root: str, nx: int, nz: int, shots: int, nt: int, niter: int, board, amp: float, method: str,
                   extra: str = "", sigma: int = 4, nrec: int | None = None, perturb: str = "both"):
-    """One inversion through the workflow; returns (optimizer, wall seconds)."""
+    """One inversion through the workflow; returns (optimizer, wall seconds,
+    true mu of the case)."""
     from . import workflow
     from .inversion_bench import write_case
-    write_case(root, nx, nz, shots, nrec or max(16, nx // 4), nt, niter, sigma, 10, board=board, amp=amp,
-               method=method, optimize_extra=extra, perturb=perturb)
+    mu_true = write_case(root, nx, nz, shots, nrec or max(16, nx // 4), nt, niter, sigma, 10, board=board, amp=amp,
+                         method=method, optimize_extra=extra, perturb=perturb)
     t0 = time.time()
     with contextlib.redirect_stdout(io.StringIO()):
         wf = workflow.main(["--workdir", os.path.join(root, "inverse")])
-    return wf.optimize, time.time() - t0
+    return wf.optimize, time.time() - t0, mu_true
 
 
 def cmd_gen(a):
@@ -113,23 +115,31 @@ def cmd_gen(a):
         amp = float(rng.uniform(0.03, 0.08))
         path = os.path.abspath(os.path.join(a.out, "pairs_%04d.npz" % c))
         with tempfile.TemporaryDirectory() as root:
-            run_inversion(root, a.nx, a.nz, a.shots, a.nt, a.niter, board, amp, "lbfgs_learned",
-                          "record_pairs = %s\n" % path, perturb=a.perturb)
+            _, _, mu_true = run_inversion(root, a.nx, a.nz, a.shots, a.nt, a.niter, board, amp, "lbfgs_learned",
+                                          "record_pairs = %s\n" % path, perturb=a.perturb)
         if os.path.exists(path):
-            npairs += len(np.load(path)["g"])
+            z = dict(np.load(path))
+            z["m_true"] = np.asarray(mu_true, np.float32).ravel()  # for the model-error target
+            np.savez(path, **z)
+            npairs += len(z["g"])
         print(json.dumps({"case": c, "pairs": npairs, "seconds": time.time() - t0}), flush=True)
         if a.max_seconds and time.time() - t0 > a.max_seconds:
             break
     print(json.dumps({"cases": c + 1, "pairs": npairs, "seconds": time.time() - t0}))
 
 
-def load_pairs(data_dir: str, device):
+def load_pairs(data_dir: str, device, target: str = "update"):
+    """Inputs and targets of every recorded iteration.  target "update": the
+    accepted L-BFGS update m_{k+1} - m_k; "error": the model error
+    m_true - m_k (synthetic cases only)."""
     X, Y = [], []
     for f in sorted(glob.glob(os.path.join(data_dir, "pairs_*.npz"))):
         z = np.load(f)
         nx, nz = int(z["nx"]), int(z["nz"])
         for k in range(len(z["g"])):
             g, i, m, d = (torch.as_tensor(z[key][k], device=device) for key in ("g", "illum", "m", "d"))
+            if target == "error":
+                d = torch.as_tensor(z["m_true"], device=device) - m
             if not float(d.abs().max()) > 0:
                 continue
             X.append(features(g, i, m, nx, nz)[0])
@@ -146,7 +156,7 @@ def _cosine(a, b):
 
 def cmd_train(a):
     dev = torch.device("cuda")
-    X, Y = load_pairs(a.data, dev)
+    X, Y = load_pairs(a.data, dev, a.target)
     n = X.shape[0]
     gen = torch.Generator().manual_seed(a.seed)
     perm = torch.randperm(n, generator=gen).to(dev)
@@ -180,7 +190,8 @@ def cmd_train(a):
         print(json.dumps(log[-1]), flush=True)
     net.save(a.weights)
     base = float((Y[val] ** 2).mean())
-    print(json.dumps({"pairs": n, "train": len(tr), "val": nval, "epochs": a.epochs, "seconds": time.time() - t0,
+    print(json.dumps({"pairs": n, "target": a.target, "train": len(tr), "val": nval, "epochs": a.epochs,
+                      "seconds": time.time() - t0,
                       "val_loss": log[-1]["val_loss"], "val_loss_zero_predictor": base,
                       "val_cosine": log[-1]["val_cosine"], "weights": a.weights}))
 
@@ -202,11 +213,13 @@ def cmd_eval(a):
     rng = np.random.default_rng(a.seed)
     board = random_board(rng, a.nx, a.nz) if a.random_model else None
     res = {}
-    for label, method, extra in (("plain", "lbfgs", ""),
-                                 ("learned", "lbfgs_learned", "unet_weights = %s\n" % os.path.abspath(a.weights))):
+    learned_extra = "unet_weights = %s\n" % os.path.abspath(a.weights)
+    if a.learned_iterations:
+        learned_extra += "learned_iterations = %d\n" % a.learned_iterations
+    for label, method, extra in (("plain", "lbfgs", ""), ("learned", "lbfgs_learned", learned_extra)):
         with tempfile.TemporaryDirectory() as root:
-            opt, wall = run_inversion(root, a.nx, a.nz, a.shots, a.nt, a.niter, board, a.amp, method, extra,
-                                      perturb=a.perturb)
+            opt, wall, _ = run_inversion(root, a.nx, a.nz, a.shots, a.nt, a.niter, board, a.amp, method, extra,
+                                         perturb=a.perturb)
         res[label] = _summary(opt, wall)
         print(json.dumps({label: res[label]}), flush=True)
     print(json.dumps({"workload": "psv_inversion_%dx%d_shots%d_nt%d_lbfgs%d_%s" % (a.nx, a.nz, a.shots, a.nt, a.niter,
@@ -242,6 +255,8 @@ def main(argv=None):
     t.add_argument("--batch", type=int, default=8)
     t.add_argument("--lr", type=float, default=1e-3)
     t.add_argument("--seed", type=int, default=0)
+    t.add_argument("--target", default="update", choices=["update", "error"],
+                   help="update: the accepted L-BFGS update; error: the true model error of the synthetic case")
     e = sub.add_parser("eval")
     e.add_argument("--weights", default=DEFAULT_WEIGHTS)
     e.add_argument("--nx", type=int, default=512)
@@ -252,6 +267,8 @@ def main(argv=None):
     e.add_argument("--amp", type=float, default=0.08)
     e.add_argument("--random-model", action="store_true", help="random board instead of the 64-cell checkerboard")
     e.add_argument("--seed", type=int, default=12345)
+    e.add_argument("--learned-iterations", type=int, default=0,
+                   help="iterations that try the learned direction (0: the optimizer's default, lbfgs_mem)")
     e.add_argument("--perturb", default="both", choices=["both", "vs", "mu"],
                    help="mu: perturb only mu (lambda kept), so that the mu-only inversion can fit the data")
     a = ap.parse_args(argv)

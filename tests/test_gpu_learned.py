@@ -26,8 +26,9 @@ def test_recorded_pairs_and_untrained_network_fallback(tmp_path):
     from seispie_b200.unet import UNet
     board = random_board(np.random.default_rng(3), NX, NZ)
     rec = str(tmp_path / "pairs.npz")
-    opt, _ = run_inversion(str(tmp_path / "a"), NX, NZ, SHOTS, NT, NITER, board, 0.06, "lbfgs_learned",
-                           "record_pairs = %s\n" % rec)
+    opt, _, mu_true = run_inversion(str(tmp_path / "a"), NX, NZ, SHOTS, NT, NITER, board, 0.06, "lbfgs_learned",
+                                    "record_pairs = %s\n" % rec)
+    assert mu_true.size == NX * NZ
     z = np.load(rec)
     n = len(z["g"])
     assert n == NITER and int(z["nx"]) == NX and int(z["nz"]) == NZ
@@ -45,8 +46,8 @@ def test_recorded_pairs_and_untrained_network_fallback(tmp_path):
     # an untrained network: the optimizer falls back where needed and still descends
     w = str(tmp_path / "w.npz")
     UNet("cuda", seed=5).save(w)
-    opt2, _ = run_inversion(str(tmp_path / "b"), NX, NZ, SHOTS, NT, NITER, board, 0.06, "lbfgs_learned",
-                            "unet_weights = %s\n" % w)
+    opt2, _, _ = run_inversion(str(tmp_path / "b"), NX, NZ, SHOTS, NT, NITER, board, 0.06, "lbfgs_learned",
+                               "unet_weights = %s\n" % w)
     mis2 = [h["misfit"] for h in opt2.history if "misfit" in h]
     assert opt2.learned_accepted + opt2.learned_rejected >= NITER - 1
     assert all(b <= a * (1 + 1e-9) for a, b in zip(mis2, mis2[1:]))
