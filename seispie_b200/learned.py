@@ -35,9 +35,12 @@ import torch
 from .unet import UNet
 
 
-# weights trained by ``gen`` + ``train`` with their defaults (1494 pairs of
-# 256 x 128 P-SV mu inversions, 30 epochs)
-DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "unet_psv_mu.npz")
+# weights trained by ``gen`` + ``train`` (about 1500 pairs of 256 x 128 P-SV mu
+# inversions, 30 epochs): on the accepted L-BFGS updates (the default), and on
+# the model error of mu-only cases (``--perturb mu``, ``--target error``)
+WEIGHTS_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights")
+DEFAULT_WEIGHTS = os.path.join(WEIGHTS_DIR, "unet_psv_mu.npz")
+ERROR_WEIGHTS = os.path.join(WEIGHTS_DIR, "unet_psv_mu_error.npz")
 
 
 def _pad8(n: int) -> int:
@@ -62,6 +65,8 @@ class Preconditioner:
 
     def __init__(self, net: UNet):
         self.net = net
+        # number of iterations the network's direction is meant for (None: the optimizer's default)
+        self.learned_iterations = getattr(net, "meta", {}).get("learned_iterations")
 
     @classmethod
     def load(cls, path: str, device="cuda") -> "Preconditioner":
@@ -188,7 +193,7 @@ def cmd_train(a):
         log.append(dict(epoch=ep, train_loss=run / len(tr), val_loss=vloss, val_cosine=float(cos.mean()),
                         val_descent_rate=desc))
         print(json.dumps(log[-1]), flush=True)
-    net.save(a.weights)
+    net.save(a.weights, target=a.target, learned_iterations=2 if a.target == "error" else 5)
     base = float((Y[val] ** 2).mean())
     print(json.dumps({"pairs": n, "target": a.target, "train": len(tr), "val": nval, "epochs": a.epochs,
                       "seconds": time.time() - t0,

@@ -4,8 +4,8 @@ The step logic is the reference's L-BFGS (optimize/lbfgs.py:5-59) with its
 backtracking line search; on top of it:
 
 * ``unet_weights = <file.npz>``: in the first ``learned_iterations``
-  iterations (default ``lbfgs_mem``: while the L-BFGS memory is still
-  short) the U-Net (seispie_b200.unet) maps (gradient, source illumination,
+  iterations (default: the number stored with the weights, else
+  ``lbfgs_mem``: while the L-BFGS memory is still short) the U-Net (seispie_b200.unet) maps (gradient, source illumination,
   model) to an update direction, scaled to the max-norm of the L-BFGS
   direction.  It is used only if it is a descent direction (g.p < 0) and its
   line search succeeds; otherwise the plain L-BFGS direction is searched
@@ -40,7 +40,8 @@ class lbfgs_learned(lbfgs):
         self.learned_accepted = 0
         self.learned_rejected = 0
         get = self.config.get if hasattr(self.config, "get") else (lambda k, d=None: d)
-        self.learned_iterations = int(get("learned_iterations", str(self.lbfgs_mem)))
+        hint = self.pre.learned_iterations if self.pre is not None else None
+        self.learned_iterations = int(get("learned_iterations", str(hint or self.lbfgs_mem)))
         self.iteration = 0
 
     def compute_direction(self):

@@ -95,10 +95,12 @@ class UNet:
     def state(self) -> dict:
         return dict(w=self.w.cpu().numpy(), step=self.step)
 
-    def save(self, path: str, optimizer_state: bool = True) -> None:
-        """Weights (and, unless optimizer_state is False, the Adam state)."""
+    def save(self, path: str, optimizer_state: bool = True, **meta) -> None:
+        """Weights (and, unless optimizer_state is False, the Adam state);
+        meta: scalar facts stored beside them (training target, suggested
+        number of learned iterations)."""
         extra = dict(m=self.m.cpu().numpy(), v=self.v.cpu().numpy(), step=self.step) if optimizer_state else {}
-        np.savez_compressed(path, w=self.w.cpu().numpy(), **extra)
+        np.savez_compressed(path, w=self.w.cpu().numpy(), **extra, **meta)
 
     @classmethod
     def load(cls, path: str, device="cuda") -> "UNet":
@@ -109,6 +111,7 @@ class UNet:
             net.m.copy_(torch.as_tensor(z["m"]))
             net.v.copy_(torch.as_tensor(z["v"]))
             net.step = int(z["step"])
+        net.meta = {k: z[k].item() for k in ("target", "learned_iterations") if k in z}
         return net
 
     # ----------------------------------------------------------- kernels
