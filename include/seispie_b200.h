@@ -122,6 +122,13 @@ int fwi_abi_version(void);
  * launch accounting by benchmarks).  No counterpart in the reference. */
 long long fwi_launch_count(void);
 
+/* Device-side status of the kernels whose waits are bounded (TMA and
+ * tensor-core pipelines): *status gets bit 0 if a step or transposed-step
+ * kernel gave up a wait, bit 1 if a U-Net kernel did (its outputs are then
+ * invalid); clear != 0 resets both.  Synchronous (reads device memory).  No
+ * counterpart in the reference. */
+int fwi_device_status(int *status, int clear);
+
 /* Copy the last error message of the calling thread into buf (always NUL
  * terminated); returns the status code of that error (0 if none). */
 int fwi_last_error(char *buf, size_t len);
@@ -301,6 +308,13 @@ int fwi_smooth(const double *in, int in_pitch, float *out, int out_pitch, double
 int fwi_unet_conv3x3(const void *in0, int c0, const void *in1, int c1, const void *w, const float *bias,
                      int cout, void *out0, int d0, void *out1, int d1, int n, int h, int wd, int relu,
                      void *stream);
+
+/* Kernel of fwi_unet_conv3x3: path 0 (default) uses the tcgen05 tensor-core
+ * kernel where wd >= 64 and the mma.sync kernel elsewhere;
+ * path 1 uses the mma.sync kernel everywhere.  Other values only query.
+ * Returns the previous path.  Process-wide; not thread-safe against
+ * concurrent convolution calls. */
+int fwi_unet_conv_path(int path);
 
 /* wd[8-tap][ci][co] = w[tap][co][ci]: the weights of the data gradient. */
 int fwi_unet_flip_weights(const void *w, void *wd, int cout, int cin, void *stream);

@@ -64,6 +64,8 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
         "fwi_abi_version": ([], ctypes.c_int),
         "fwi_launch_count": ([], ctypes.c_longlong),
         "fwi_last_error": ([ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
+        "fwi_device_status": ([ctypes.POINTER(ctypes.c_int), ctypes.c_int], ctypes.c_int),
+        "fwi_unet_conv_path": ([ctypes.c_int], ctypes.c_int),
         "fwi_tile_shape": ([ctypes.c_int, _ip, _ip], ctypes.c_int),
         "fwi_tile_kind": ([ctypes.c_int], ctypes.c_int),
         "fwi_vps2lm": ([_vp, _vp, _vp, ctypes.c_longlong, _vp], ctypes.c_int),

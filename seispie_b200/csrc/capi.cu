@@ -127,6 +127,16 @@ int fwi_abi_version(void) { return FWI_ABI_VERSION; }
 
 long long fwi_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
+int fwi_device_status(int *status, int clear) {
+    if (!status) return set_error(FWI_EINVAL, "fwi_device_status: NULL status");
+    int a = 0, b = 0;
+    int rc = step_device_status(clear, &a);
+    if (!rc) rc = unet_device_status(clear, &b);
+    if (rc) return rc;
+    *status = (a ? 1 : 0) | (b ? 2 : 0);
+    return 0;
+}
+
 int fwi_last_error(char *buf, size_t len) {
     if (buf && len) {
         strncpy(buf, g_msg, len - 1);

@@ -221,50 +221,22 @@ struct TmaMaps {
     CUtensorMap ip[4];  // model fields read on the interior
 };
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, int count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Bounded wait: gives up after ~2^22 polls (each poll may suspend the warp
-// for a while), so a lost transaction ends the kernel instead of hanging it.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-    for (int i = 0; i < (1 << 22); i++)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int c0, int c1, int c2,
-                                            uint64_t *bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::
-            "r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
-        : "memory");
-}
-__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int c0, int c1, uint64_t *bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
-            smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_u32(bar))
-        : "memory");
-}
-
 // Device-side status of the TMA kernels (a wait that gave up), read and
 // cleared by fwi_device_status.
 __device__ int g_device_status = 0;
+
+int step_device_status(int clear, int *status) {
+    int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_device_status, sizeof(int)) != cudaSuccess)
+        return set_error(FWI_ECUDA, "fwi_device_status: reading the step kernels' status failed");
+    if (clear && v) {
+        const int z = 0;
+        if (cudaMemcpyToSymbol(g_device_status, &z, sizeof(int)) != cudaSuccess)
+            return set_error(FWI_ECUDA, "fwi_device_status: clearing the step kernels' status failed");
+    }
+    *status = v;
+    return 0;
+}
 
 // Staging copies plus the source scatter (stf_dsy / stf_dsxz, solver.py:78-93):
 // entries of this shot inside the computed velocity region are summed per
@@ -732,26 +704,6 @@ struct TileShape {
 static const TileShape kTiles[] = {{32, 32, 2}, {32, 32, 0}, {16, 64, 0}, {16, 32, 0}, {64, 32, 0}, {8, 64, 0},
                                    {32, 32, 1}, {16, 32, 1}, {64, 32, 1}, {32, 32, 2}, {16, 32, 2}, {8, 32, 2}};
 constexpr int kNumTiles = sizeof(kTiles) / sizeof(kTiles[0]);
-
-// cuTensorMapEncodeTiled, fetched from the driver at run time.
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-static EncodeTiledFn encode_fn() {
-    static EncodeTiledFn fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
-        void *p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
-                cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiledFn>(p);
-    }
-    return fn;
-}
 
 // Tiled float32 map over a [nshots][nx][pitch] block (rank 3) or an
 // [nx][pitch] model array (rank 2), box (bz, bx), zero fill outside.

@@ -158,6 +158,226 @@ __global__ void __launch_bounds__(kCT) conv3x3_kernel(const bf16 *in0, int c0, c
     }
 }
 
+// ---------------------------------------------------------------------------
+// The same convolution on the 5th-generation tensor cores (tcgen05.mma, FP32
+// accumulator in tensor memory).  The halo box may reach past the image on
+// every side (images narrower than a strip, or fewer than 3 rows high): the
+// tensor map fills what lies outside with zeros.
+//
+// A CTA owns a strip of kStrip = 128 consecutive pixels of one image row and
+// BN output channels.  Per 16-channel chunk of the (concatenated) input, TMA
+// brings the strip's 3 x 130 halo (rows y-1..y+1, columns x0-1..x0+128; zero
+// outside the image from the tensor map) into shared memory once, as two
+// planes of 8 channels ([row][column][8] bf16, 16 bytes per pixel), with the
+// chunk's weights of all 9 taps ([tap][BN][8] per plane).  The 9 taps are 9
+// MMAs (M = 128 pixels, N = BN, K = 16) whose A operand is that one halo tile
+// seen from a shifted start: pixel r of tap (dy, dx) sits at
+// plane + ((dy+1)*130 + r + dx + 1)*16, which is the K-major, no-swizzle
+// canonical layout (8-row core matrices of 16-byte rows, 128 bytes apart =
+// SBO; the second 8-channel plane LBO bytes further).  No per-tap restaging.
+//
+// Roles: warp 1 lane 0 issues the TMA copies into a ring of stages, warp 0
+// lane 0 issues the MMAs and hands each stage back to the producer with
+// tcgen05.commit on an mbarrier; then all four warps read the accumulator
+// (tensor-memory lane = pixel, column = output channel) and write
+// bias + ReLU + bf16.  Every wait is bounded; a wait that gives up sets
+// g_unet_status, lets the copies in flight land and still frees the tensor
+// memory.
+constexpr int kStrip = 128;                                // pixels per CTA (MMA M)
+constexpr int kHaloW = kStrip + 2;                         // staged columns
+constexpr int kPlaneA = 3 * kHaloW * 16;                   // bytes of one 8-channel halo plane
+constexpr int kPlaneAPad = (kPlaneA + 127) / 128 * 128;    // planes start 128-byte aligned
+constexpr int kTcHead = 256;                               // mbarriers, tensor-memory address, flags
+
+template <int BN>
+struct TcConv {
+    static constexpr int kPlaneB = 9 * BN * 16;            // one 8-channel plane of the 9 taps' weights
+    static constexpr int kStage = 2 * kPlaneAPad + 2 * kPlaneB;
+    static constexpr int kStages = BN >= 128 ? 2 : BN >= 64 ? 3 : 4;
+    static constexpr int kTmemCols = BN < 32 ? 32 : BN;    // power of two >= 32
+    static constexpr uint32_t kTx = 2 * kPlaneA + 2 * kPlaneB;  // bytes the copies of one stage deliver
+    static constexpr int kSmemMax = kTcHead + 128 + kStages * kStage;
+    static_assert(kTx < (1u << 20), "mbarrier transaction count limit");
+    static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "MMA N for M = 128");
+};
+
+struct TcMaps {
+    CUtensorMap in0, in1, wt;
+};
+
+__device__ int g_unet_status = 0;
+
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];\n" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+        : "memory");
+}
+// Shared-memory matrix descriptor of tcgen05.mma, K-major without swizzle:
+// start address, leading byte offset (distance of the two 8-element K
+// halves), stride byte offset (distance of 8-row core matrices), version 1.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// Instruction descriptor of kind::f16: D f32, A and B bf16, both K-major, M = 128.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+            tmem_d),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_ld16(uint32_t (&r)[16], uint32_t taddr) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+template <int BN>
+__global__ void __launch_bounds__(128) conv3x3_tc_kernel(const __grid_constant__ TcMaps maps, int c0, int nck,
+                                                         const float *bias, bf16 *out0, int d0, bf16 *out1, int d1,
+                                                         Shape s, int strips, int relu) {
+    using C = TcConv<BN>;
+    extern __shared__ uint8_t tc_smem[];
+    uint8_t *base = tc_smem + ((128u - (smem_u32(tc_smem) & 127u)) & 127u);
+    uint64_t *full = reinterpret_cast<uint64_t *>(base);  // [kStages]: copies landed
+    uint64_t *empty = full + C::kStages;                  // [kStages]: MMAs done reading
+    uint64_t *done = empty + C::kStages;                  // every MMA done
+    volatile int *info = reinterpret_cast<volatile int *>(done + 1);  // tmem address, error, issued, consumed
+    uint8_t *stage0 = base + kTcHead;
+    const int nst = nck < C::kStages ? nck : C::kStages;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int row = blockIdx.x / strips;  // n*h + y
+    const int x0 = (blockIdx.x - row * strips) * kStrip;
+    const int img = row / s.h, y = row - img * s.h;
+    const int co0 = blockIdx.y * BN;
+    if (tid == 0) {
+        for (int i = 0; i < nst; i++) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        mbar_init(done, 1);
+        info[1] = 0;
+        info[2] = 0;
+        info[3] = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32((const void *)&info[0])),
+                     "r"(C::kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = (uint32_t)info[0];
+
+    if (warp == 1 && lane == 0) {  // producer
+        int c = 0;
+        for (; c < nck; c++) {
+            const int st = c % nst;
+            if (c >= nst && !mbar_wait(&empty[st], ((c / nst) - 1) & 1)) {
+                info[1] = 1;
+                break;
+            }
+            uint8_t *sp = stage0 + st * C::kStage;
+            mbar_expect_tx(&full[st], C::kTx);
+            const int ch = c * 16;
+            const CUtensorMap *m = ch < c0 ? &maps.in0 : &maps.in1;
+            const int cc = ch < c0 ? ch : ch - c0;
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                tma_load_4d(sp + j * kPlaneAPad, m, cc + 8 * j, x0 - 1, y - 1, img, &full[st]);
+                tma_load_3d(sp + 2 * kPlaneAPad + j * C::kPlaneB, &maps.wt, ch + 8 * j, co0, 0, &full[st]);
+            }
+        }
+        info[2] = c;
+    }
+    if (warp == 0 && lane == 0) {  // MMA issuer
+        constexpr uint32_t idesc = umma_idesc_bf16(BN);
+        int c = 0;
+        for (; c < nck; c++) {
+            const int st = c % nst;
+            if (!mbar_wait(&full[st], (c / nst) & 1)) {
+                info[1] = 1;
+                break;
+            }
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(stage0 + st * C::kStage), b0 = a0 + 2 * kPlaneAPad;
+#pragma unroll
+            for (int t = 0; t < 9; t++) {
+                const uint64_t ad = umma_desc(a0 + ((t / 3) * kHaloW + t % 3) * 16, kPlaneAPad, 128);
+                const uint64_t bd = umma_desc(b0 + t * BN * 16, C::kPlaneB, 128);
+                umma_bf16(tmem, ad, bd, idesc, (c | t) != 0);
+            }
+            umma_commit(&empty[st]);
+        }
+        info[3] = c;
+        umma_commit(done);  // arrives once every MMA issued above has completed
+    }
+    __syncwarp();
+    if (!mbar_wait(done, 0)) info[1] = 1;
+    __syncthreads();
+    if (info[1]) {
+        if (tid == 32)  // copies issued but never consumed: one bounded chance to land
+            for (int c = info[3]; c < info[2]; c++) mbar_wait(&full[c % nst], (c / nst) & 1);
+        if (tid == 0) atomicExch(&g_unet_status, 1);
+    } else {
+        tc_fence_after();
+        const int x = x0 + warp * 32 + lane;
+        const long long p = (long long)row * s.w + x;
+#pragma unroll 1
+        for (int g = 0; g < BN / 16; g++) {
+            uint32_t r[16];
+            tmem_ld16(r, tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(g * 16));
+            if (x >= s.w) continue;  // after the warp-wide load
+            const int co = co0 + g * 16;
+            uint32_t packed[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                float v0 = __uint_as_float(r[2 * i]), v1 = __uint_as_float(r[2 * i + 1]);
+                if (bias) {
+                    v0 += bias[co + 2 * i];
+                    v1 += bias[co + 2 * i + 1];
+                }
+                if (relu) {
+                    v0 = fmaxf(v0, 0.f);
+                    v1 = fmaxf(v1, 0.f);
+                }
+                const __nv_bfloat162 b2 = __floats2bfloat162_rn(v0, v1);
+                packed[i] = *reinterpret_cast<const uint32_t *>(&b2);
+            }
+            bf16 *dst = co < d0 ? out0 + p * d0 + co : out1 + p * d1 + (co - d0);
+            uint4 *d4 = reinterpret_cast<uint4 *>(dst);
+            d4[0] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+            d4[1] = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(C::kTmemCols)
+                     : "memory");
+    }
+}
+
 // Weights of the data gradient: wd[8-tap][ci][co] = w[tap][co][ci].
 __global__ void flip_weights_kernel(const bf16 *w, bf16 *wd, int cout, int cin) {
     const long long n = 9ll * cout * cin;
@@ -428,6 +648,87 @@ static bool a16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
 using namespace fwi;
 using namespace fwi::unet;
 
+// Convolution kernel selection: 0 = tcgen05 where the image is at least
+// kTcMinWidth pixels wide (mma.sync otherwise), 1 = mma.sync only.  Narrower
+// images would leave most of the 128 MMA rows of a strip empty.
+constexpr int kTcMinWidth = 64;
+static int g_conv_path = 0;
+
+// bf16 tiled tensor map, zero fill outside; dims innermost first, strides in
+// bytes of dims 1..rank-1.
+static int encode_bf16(CUtensorMap *m, const void *base, int rank, const cuuint64_t *dims, const cuuint64_t *strides,
+                       const cuuint32_t *box) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return set_error(FWI_ECUDA, "cuTensorMapEncodeTiled unavailable from the driver");
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, (cuuint32_t)rank, const_cast<void *>(base), dims, strides, box,
+                    es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(FWI_ECUDA, "cuTensorMapEncodeTiled (bf16) failed (%d)", (int)r);
+    return 0;
+}
+
+// Halo map of an NHWC activation: dims (c, w, h, n), box 8 x kHaloW x 3 x 1.
+static int encode_act(CUtensorMap *m, const bf16 *x, int c, const Shape &s) {
+    const cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)s.w, (cuuint64_t)s.h, (cuuint64_t)s.n};
+    const cuuint64_t strides[3] = {(cuuint64_t)c * 2, (cuuint64_t)c * 2 * s.w, (cuuint64_t)c * 2 * s.w * s.h};
+    const cuuint32_t box[4] = {8, (cuuint32_t)kHaloW, 3, 1};
+    return encode_bf16(m, x, 4, dims, strides, box);
+}
+
+template <int BN>
+static int launch_tc(const TcMaps &maps, int c0, int nck, const float *bias, bf16 *o0, int d0, bf16 *o1, int d1,
+                     const Shape &s, int relu, int cout, cudaStream_t st) {
+    using C = TcConv<BN>;
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(conv3x3_tc_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::kSmemMax) !=
+            cudaSuccess)
+            return set_error(FWI_ECUDA, "unet_conv3x3: shared-memory attribute refused");
+        attr = true;
+    }
+    const int strips = (s.w + kStrip - 1) / kStrip;
+    const long long blocks = (long long)s.n * s.h * strips;
+    if (blocks >= 0x7fffffffll) return set_error(FWI_ERANGE, "fwi_unet_conv3x3: too many pixel strips");
+    const int nst = nck < C::kStages ? nck : C::kStages;
+    const size_t smem = kTcHead + 128 + (size_t)nst * C::kStage;
+    conv3x3_tc_kernel<BN><<<dim3((unsigned)blocks, cout / BN), 128, smem, st>>>(maps, c0, nck, bias, o0, d0, o1, d1, s,
+                                                                               strips, relu);
+    return check_launch("unet_conv3x3 (tcgen05)");
+}
+
+static int conv3x3_tc(const bf16 *i0, int c0, const bf16 *i1, int c1, const bf16 *wt, const float *bias, int cout,
+                      bf16 *o0, int d0, bf16 *o1, int d1, const Shape &s, int relu, cudaStream_t st) {
+    const int ct = c0 + c1;
+    const int bn = cout % 128 == 0 ? 128 : cout % 64 == 0 ? 64 : cout % 32 == 0 ? 32 : 16;
+    TcMaps maps;
+    int rc = encode_act(&maps.in0, i0, c0, s);
+    if (!rc) rc = c1 ? encode_act(&maps.in1, i1, c1, s) : encode_act(&maps.in1, i0, c0, s);
+    const cuuint64_t wdims[3] = {(cuuint64_t)ct, (cuuint64_t)cout, 9};
+    const cuuint64_t wstr[2] = {(cuuint64_t)ct * 2, (cuuint64_t)ct * 2 * cout};
+    const cuuint32_t wbox[3] = {8, (cuuint32_t)bn, 9};
+    if (!rc) rc = encode_bf16(&maps.wt, wt, 3, wdims, wstr, wbox);
+    if (rc) return rc;
+    const int nck = ct / 16;
+    if (bn == 128) return launch_tc<128>(maps, c0, nck, bias, o0, d0, o1, d1, s, relu, cout, st);
+    if (bn == 64) return launch_tc<64>(maps, c0, nck, bias, o0, d0, o1, d1, s, relu, cout, st);
+    if (bn == 32) return launch_tc<32>(maps, c0, nck, bias, o0, d0, o1, d1, s, relu, cout, st);
+    return launch_tc<16>(maps, c0, nck, bias, o0, d0, o1, d1, s, relu, cout, st);
+}
+
+int fwi::unet_device_status(int clear, int *status) {
+    int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_unet_status, sizeof(int)) != cudaSuccess)
+        return set_error(FWI_ECUDA, "fwi_device_status: reading the U-Net kernels' status failed");
+    if (clear && v) {
+        const int z = 0;
+        if (cudaMemcpyToSymbol(g_unet_status, &z, sizeof(int)) != cudaSuccess)
+            return set_error(FWI_ECUDA, "fwi_device_status: clearing the U-Net kernels' status failed");
+    }
+    *status = v;
+    return 0;
+}
+
 #define UREQ(cond, ...)                                        \
     do {                                                       \
         if (!(cond)) return set_error(FWI_EINVAL, __VA_ARGS__); \
@@ -447,15 +748,23 @@ int fwi_unet_conv3x3(const void *in0, int c0, const void *in1, int c1, const voi
     const long long npix = (long long)n * h * wd;
     UREQ(npix / kBM < 0x7fffffffll, "fwi_unet_conv3x3: too many pixels");
     const Shape s{n, h, wd};
-    const int bn = cout % 64 == 0 ? 64 : cout % 32 == 0 ? 32 : 16;
-    dim3 grid((unsigned)((npix + kBM - 1) / kBM), cout / bn);
     cudaStream_t st = (cudaStream_t)stream;
     const bf16 *i0 = (const bf16 *)in0, *i1 = (const bf16 *)in1, *wt = (const bf16 *)w;
     bf16 *o0 = (bf16 *)out0, *o1 = (bf16 *)out1;
+    if (g_conv_path == 0 && wd >= kTcMinWidth)
+        return conv3x3_tc(i0, c0, i1, c1, wt, bias, cout, o0, d0, o1, d1, s, relu, st);
+    const int bn = cout % 64 == 0 ? 64 : cout % 32 == 0 ? 32 : 16;
+    dim3 grid((unsigned)((npix + kBM - 1) / kBM), cout / bn);
     if (bn == 64) conv3x3_kernel<64><<<grid, kCT, 0, st>>>(i0, c0, i1, c1, wt, bias, cout, o0, d0, o1, d1, s, relu);
     else if (bn == 32) conv3x3_kernel<32><<<grid, kCT, 0, st>>>(i0, c0, i1, c1, wt, bias, cout, o0, d0, o1, d1, s, relu);
     else conv3x3_kernel<16><<<grid, kCT, 0, st>>>(i0, c0, i1, c1, wt, bias, cout, o0, d0, o1, d1, s, relu);
     return check_launch("unet_conv3x3");
+}
+
+int fwi_unet_conv_path(int path) {
+    const int old = g_conv_path;
+    if (path == 0 || path == 1) g_conv_path = path;
+    return old;
 }
 
 int fwi_unet_flip_weights(const void *w, void *wd, int cout, int cin, void *stream) {

@@ -247,8 +247,9 @@ class UNet:
 
 
 def bench(h: int = 2048, w: int = 1024, reps: int = 20) -> list:
-    """TFLOP/s of the 3x3 convolution (forward, data and weight gradients) at
-    the four U-Net levels of an h x w image (CUDA events, after warm-up)."""
+    """TFLOP/s of the 3x3 convolution (forward and data gradient on the
+    tcgen05 and on the mma.sync kernel, weight gradient) at the four U-Net
+    levels of an h x w image (CUDA events, after warm-up)."""
     from .engine import check, ptr, stream_handle
     lib = _lib.load()
     dev = torch.device("cuda")
@@ -259,34 +260,45 @@ def bench(h: int = 2048, w: int = 1024, reps: int = 20) -> list:
         x = torch.randn(1, hh, ww, c, device=dev).to(torch.bfloat16)
         wt = (torch.randn(9 * c * c, device=dev) * 0.05).to(torch.bfloat16)
         wd = torch.empty_like(wt)
+        check(lib.fwi_unet_flip_weights(ptr(wt), ptr(wd), c, c, st), "flip")
         y = torch.empty_like(x)
         b = torch.zeros(c, device=dev)
         part = torch.empty(lib.fwi_unet_wgrad_partials(c, c, 1, hh, ww), device=dev)
         dw = torch.empty(9 * c * c, device=dev)
         flops = 2.0 * hh * ww * 9 * c * c
         res = dict(level=lvl, image=[hh, ww], channels=c)
-        for name, fn in (
-                ("fwd", lambda: lib.fwi_unet_conv3x3(ptr(x), c, None, 0, ptr(wt), ptr(b), c, ptr(y), c, None, 0, 1, hh,
-                                                     ww, 1, st)),
-                ("dgrad", lambda: lib.fwi_unet_conv3x3(ptr(x), c, None, 0, ptr(wd), None, c, ptr(y), c, None, 0, 1,
-                                                       hh, ww, 0, st)),
-                ("wgrad", lambda: lib.fwi_unet_conv3x3_wgrad(ptr(x), c, ptr(y), c, None, 0, 1, hh, ww, ptr(part),
-                                                             ptr(dw), None, st))):
-            for _ in range(3):
-                check(fn(), name)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            for _ in range(reps):
-                fn()
-            e1.record()
-            torch.cuda.synchronize()
+        cases = []
+        for path, tag in ((0, ""), (1, "_mma_sync")):
+            cases += [("fwd" + tag, path, lambda: lib.fwi_unet_conv3x3(ptr(x), c, None, 0, ptr(wt), ptr(b), c, ptr(y), c,
+                                                                       None, 0, 1, hh, ww, 1, st)),
+                      ("dgrad" + tag, path, lambda: lib.fwi_unet_conv3x3(ptr(y), c, None, 0, ptr(wd), None, c, ptr(x), c,
+                                                                         None, 0, 1, hh, ww, 0, st))]
+        cases.append(("wgrad", 0, lambda: lib.fwi_unet_conv3x3_wgrad(ptr(x), c, ptr(y), c, None, 0, 1, hh, ww,
+                                                                     ptr(part), ptr(dw), None, st)))
+        for name, path, fn in cases:
+            old = lib.fwi_unet_conv_path(path)
+            try:
+                for _ in range(3):
+                    check(fn(), name)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(reps):
+                    fn()
+                e1.record()
+                torch.cuda.synchronize()
+            finally:
+                lib.fwi_unet_conv_path(old)
             ms = e0.elapsed_time(e1) / reps
-            res[name + "_us"] = ms * 1e3
-            res[name + "_tflops"] = flops / (ms * 1e-3) / 1e12
+            res[name + "_us"] = round(ms * 1e3, 2)
+            res[name + "_tflops"] = round(flops / (ms * 1e-3) / 1e12, 1)
         out.append(res)
     return out
 
 
 if __name__ == "__main__":
+    # python -m seispie_b200.unet [rows columns [repetitions]]
     import json
-    print(json.dumps(bench()))
+    import sys
+    args = [int(a) for a in sys.argv[1:4]]
+    for r in bench(*args):
+        print(json.dumps(r))

@@ -79,6 +79,49 @@ def test_conv3x3_forward_data_and_weight_gradients():
     assert _relerr(db, gy_masked.sum((0, 1, 2))) < 1e-5
 
 
+@pytest.mark.parametrize("n,h,w,c0,c1,co,d1", [
+    (2, 5, 260, 32, 16, 48, 16),    # two full strips and a 4-pixel one; concatenated input; split output
+    (1, 4, 130, 16, 0, 16, 0),      # exactly one halo box wide, one chunk
+    (3, 2, 64, 32, 0, 32, 0),       # narrowest image of the tcgen05 path, 2 rows: box past every edge
+    (2, 1, 100, 16, 16, 32, 0),     # one row
+    (1, 3, 200, 128, 0, 128, 0),    # N = 128, ring of 2 stages wrapped 4 times
+    (2, 6, 140, 128, 64, 64, 0),    # N = 64, 12 chunks through a ring of 3
+    (1, 7, 131, 64, 32, 32, 0),     # N = 32, 6 chunks through a ring of 4
+])
+def test_conv3x3_tcgen05_matches_torch_and_mma_sync(n, h, w, c0, c1, co, d1):
+    """The tcgen05 kernel (images >= 130 pixels wide) against torch fp32 and
+    against the mma.sync kernel on the same bf16 values."""
+    from seispie_b200 import _lib
+    from seispie_b200.engine import check, ptr, stream_handle
+    import ctypes
+    lib, st = _lib.load(), stream_handle(None)
+    g = torch.Generator(device="cuda").manual_seed(11 + w)
+    x0 = _bf(torch.randn(n, h, w, c0, device="cuda", generator=g)).bfloat16()
+    x1 = _bf(torch.randn(n, h, w, max(c1, 16), device="cuda", generator=g)).bfloat16()
+    wt = _bf(torch.randn(9, co, c0 + c1, device="cuda", generator=g) * 0.1).bfloat16()
+    b = torch.randn(co, device="cuda", generator=g)
+    d0 = co - d1
+    outs = []
+    for path in (0, 1):
+        old = lib.fwi_unet_conv_path(path)
+        o0 = torch.full((n, h, w, d0), float("nan"), dtype=torch.bfloat16, device="cuda")
+        o1 = torch.full((n, h, w, max(d1, 16)), float("nan"), dtype=torch.bfloat16, device="cuda")
+        check(lib.fwi_unet_conv3x3(ptr(x0), c0, ptr(x1) if c1 else None, c1, ptr(wt), ptr(b), co, ptr(o0), d0,
+                                   ptr(o1) if d1 else None, d1, n, h, w, 1, st), "conv path %d" % path)
+        lib.fwi_unet_conv_path(old)
+        outs.append(torch.cat([o0.float(), o1[..., :d1].float()], -1))
+    torch.cuda.synchronize()
+    status = ctypes.c_int(-1)
+    check(lib.fwi_device_status(ctypes.byref(status), 1), "status")
+    assert status.value == 0
+    xt = torch.cat([x0.float(), x1[..., :c1].float()], -1).permute(0, 3, 1, 2)
+    ref = F.relu(F.conv2d(xt, _torch_w(wt.float(), co, c0 + c1), b, padding=1)).permute(0, 2, 3, 1)
+    for got in outs:
+        assert torch.isfinite(got).all()
+        assert (got - ref).abs().max() <= 1e-2 * ref.abs().max()
+    assert (outs[0] - outs[1]).abs().max() <= 1e-2 * ref.abs().max()
+
+
 def test_pool_upsample_pack_head():
     from seispie_b200 import _lib
     from seispie_b200.engine import check, ptr, stream_handle
@@ -154,11 +197,14 @@ def _torch_unet(net, planes):
     return out, P, hw, hb
 
 
-def test_unet_forward_backward_match_torch_and_training_reduces_loss():
+@pytest.mark.parametrize("h,w,train", [(32, 48, True), (16, 512, False)])
+def test_unet_forward_backward_match_torch_and_training_reduces_loss(h, w, train):
+    """48 pixels wide: every convolution on the mma.sync kernel; 512 wide:
+    every one on the tcgen05 kernel (level widths 512 to 64)."""
     from seispie_b200.unet import LAYERS, UNet
     net = UNet("cuda", seed=1)
     g = torch.Generator(device="cuda").manual_seed(7)
-    n, h, w = 2, 32, 48
+    n = 2
     planes = torch.randn(n, 3, h, w, device="cuda", generator=g)
     target = torch.randn(n, h, w, device="cuda", generator=g)
     out = net.forward(planes)
@@ -177,6 +223,8 @@ def test_unet_forward_backward_match_torch_and_training_reduces_loss():
         assert _relerr(gw, gw_ref) < 5e-2, name
         assert _relerr(net.view(name + ".b", net.g), P[name][1].grad) < 5e-2, name
     assert _relerr(net.view("head.w", net.g), hw.grad) < 2e-2
+    if not train:
+        return
     # a few Adam steps on one batch drive the loss down
     l0 = float(loss)
     for _ in range(60):
