@@ -436,7 +436,7 @@ template <int MODE, int TX, int TZ>
 __device__ __forceinline__ bool velocity_cell(const StepArgs &a, const Smem<MODE, TX, TZ> &sm, int x0, int z0, int rx,
                                               int rz, bool has_inj, float (&v)[3], float (&ds)[3]) {
     using T = Tile<MODE, TX, TZ>;
-    constexpr int SX = T::SX, SZ = T::SZ, VX = T::VX;
+    constexpr int SZ = T::SZ;
     const int gx = x0 - 1 + rx, gz = z0 - 1 + rz;
     const int cz = rz + 3;
     if (gx < 0 || gx >= a.nx || gz < 0 || gz >= a.nz) {
@@ -491,7 +491,7 @@ __device__ __forceinline__ void velocity_halo(const StepArgs &a, const Smem<MODE
 template <int MODE, int TX, int TZ>
 __global__ void __launch_bounds__(kThreads, MODE == FWI_SPIN ? 1 : 2) step_kernel(const StepArgs a) {
     using T = Tile<MODE, TX, TZ>;
-    constexpr int SX = T::SX, SZ = T::SZ, VX = T::VX;
+    constexpr int SX = T::SX, SZ = T::SZ;
     extern __shared__ __align__(128) float smem[];
     const Smem<MODE, TX, TZ> sm(smem);
     const int z0 = blockIdx.x * TZ, x0 = blockIdx.y * TX, shot = blockIdx.z;
@@ -554,7 +554,7 @@ __device__ __forceinline__ void rw_body(const StepArgs &a, const TmaMaps &maps, 
     static_assert(RPW >= 1 && RPW * (kThreads / 32) == TX, "TX must be a multiple of the warp count");
     using T = Tile<MODE, TX, TZ>;
     using F = Fields<MODE>;
-    constexpr int SX = T::SX, SZ = T::SZ, VX = T::VX;
+    constexpr int SZ = T::SZ;
     const Smem<MODE, TX, TZ> sm(smem);
     const int nx = a.nx, nz = a.nz, pitch = a.pitch;
     const long long soff = (long long)shot * nx * pitch;

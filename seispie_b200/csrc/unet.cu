@@ -164,41 +164,48 @@ __global__ void __launch_bounds__(kCT) conv3x3_kernel(const bf16 *in0, int c0, c
 // every side (images narrower than a strip, or fewer than 3 rows high): the
 // tensor map fills what lies outside with zeros.
 //
-// A CTA owns a strip of kStrip = 128 consecutive pixels of one image row and
-// BN output channels.  Per 16-channel chunk of the (concatenated) input, TMA
-// brings the strip's 3 x 130 halo (rows y-1..y+1, columns x0-1..x0+128; zero
-// outside the image from the tensor map) into shared memory once, as two
-// planes of 8 channels ([row][column][8] bf16, 16 bytes per pixel), with the
-// chunk's weights of all 9 taps ([tap][BN][8] per plane).  The 9 taps are 9
-// MMAs (M = 128 pixels, N = BN, K = 16) whose A operand is that one halo tile
-// seen from a shifted start: pixel r of tap (dy, dx) sits at
-// plane + ((dy+1)*130 + r + dx + 1)*16, which is the K-major, no-swizzle
-// canonical layout (8-row core matrices of 16-byte rows, 128 bytes apart =
-// SBO; the second 8-channel plane LBO bytes further).  No per-tap restaging.
+// A CTA owns R strips of kStrip = 128 consecutive pixels (the same columns
+// of R consecutive image rows) and BN output channels.  Per 16-channel chunk
+// of the (concatenated) input, TMA brings the (R + 2) x 130 halo (rows
+// y0-1..y0+R, columns x0-1..x0+128; zero outside the image from the tensor
+// map) into shared memory once, as two planes of 8 channels ([row][column][8]
+// bf16, 16 bytes per pixel), with the chunk's weights of all 9 taps
+// ([tap][BN][8] per plane).  Row r's 9 taps are 9 MMAs (M = 128 pixels,
+// N = BN, K = 16) into its own accumulator columns, whose A operand is that
+// one halo tile seen from a shifted start: pixel i of tap (dy, dx) sits at
+// plane + ((r + dy + 1)*130 + i + dx + 1)*16, which is the K-major,
+// no-swizzle canonical layout (8-row core matrices of 16-byte rows, 128
+// bytes apart = SBO; the second 8-channel plane LBO bytes further).  No
+// per-tap restaging, and neighbouring rows share their halo rows and the
+// weights.  (The copies arrive in 16-byte pieces, one per pixel and plane,
+// because channels are innermost in memory; the TMA unit's rate for such
+// pieces, not the tensor cores, bounds the kernel, hence R > 1.)
 //
 // Roles: warp 1 lane 0 issues the TMA copies into a ring of stages, warp 0
 // lane 0 issues the MMAs and hands each stage back to the producer with
 // tcgen05.commit on an mbarrier; then all four warps read the accumulator
-// (tensor-memory lane = pixel, column = output channel) and write
+// (tensor-memory lane = pixel, column = row * BN + output channel) and write
 // bias + ReLU + bf16.  Every wait is bounded; a wait that gives up sets
 // g_unet_status, lets the copies in flight land and still frees the tensor
 // memory.
-constexpr int kStrip = 128;                                // pixels per CTA (MMA M)
+constexpr int kStrip = 128;                                // pixels per strip (MMA M)
 constexpr int kHaloW = kStrip + 2;                         // staged columns
-constexpr int kPlaneA = 3 * kHaloW * 16;                   // bytes of one 8-channel halo plane
-constexpr int kPlaneAPad = (kPlaneA + 127) / 128 * 128;    // planes start 128-byte aligned
 constexpr int kTcHead = 256;                               // mbarriers, tensor-memory address, flags
 
 template <int BN>
 struct TcConv {
+    static constexpr int R = BN >= 128 ? 2 : 4;           // image rows per CTA
+    static constexpr int kPlaneA = (R + 2) * kHaloW * 16;  // bytes of one 8-channel halo plane
+    static constexpr int kPlaneAPad = (kPlaneA + 127) / 128 * 128;  // planes start 128-byte aligned
     static constexpr int kPlaneB = 9 * BN * 16;            // one 8-channel plane of the 9 taps' weights
     static constexpr int kStage = 2 * kPlaneAPad + 2 * kPlaneB;
-    static constexpr int kStages = BN >= 128 ? 2 : BN >= 64 ? 3 : 4;
-    static constexpr int kTmemCols = BN < 32 ? 32 : BN;    // power of two >= 32
+    static constexpr int kStages = BN >= 64 ? 2 : 3;
+    static constexpr int kTmemCols = R * BN <= 32 ? 32 : R * BN <= 64 ? 64 : R * BN <= 128 ? 128 : 256;
     static constexpr uint32_t kTx = 2 * kPlaneA + 2 * kPlaneB;  // bytes the copies of one stage deliver
     static constexpr int kSmemMax = kTcHead + 128 + kStages * kStage;
     static_assert(kTx < (1u << 20), "mbarrier transaction count limit");
     static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "MMA N for M = 128");
+    static_assert(R * BN <= kTmemCols && R + 2 <= 256, "accumulator columns, box rows");
 };
 
 struct TcMaps {
@@ -250,7 +257,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t (&r)[16], uint32_t taddr) {
 template <int BN>
 __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const __grid_constant__ TcMaps maps, int c0, int nck,
                                                          const float *bias, bf16 *out0, int d0, bf16 *out1, int d1,
-                                                         Shape s, int strips, int relu) {
+                                                         Shape s, int strips, int groups, int relu) {
     using C = TcConv<BN>;
     extern __shared__ uint8_t tc_smem[];
     uint8_t *base = tc_smem + ((128u - (smem_u32(tc_smem) & 127u)) & 127u);
@@ -261,9 +268,10 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const __grid_constant__
     uint8_t *stage0 = base + kTcHead;
     const int nst = nck < C::kStages ? nck : C::kStages;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int row = blockIdx.x / strips;  // n*h + y
-    const int x0 = (blockIdx.x - row * strips) * kStrip;
-    const int img = row / s.h, y = row - img * s.h;
+    constexpr int R = C::R;
+    const int t_ = blockIdx.x / strips;  // image * groups + row group
+    const int x0 = (blockIdx.x - t_ * strips) * kStrip;
+    const int img = t_ / groups, y0 = (t_ - img * groups) * R;
     const int co0 = blockIdx.y * BN;
     if (tid == 0) {
         for (int i = 0; i < nst; i++) {
@@ -303,8 +311,8 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const __grid_constant__
             const int cc = ch < c0 ? ch : ch - c0;
 #pragma unroll
             for (int j = 0; j < 2; j++) {
-                tma_load_4d(sp + j * kPlaneAPad, m, cc + 8 * j, x0 - 1, y - 1, img, &full[st]);
-                tma_load_3d(sp + 2 * kPlaneAPad + j * C::kPlaneB, &maps.wt, ch + 8 * j, co0, 0, &full[st]);
+                tma_load_4d(sp + j * C::kPlaneAPad, m, cc + 8 * j, x0 - 1, y0 - 1, img, &full[st]);
+                tma_load_3d(sp + 2 * C::kPlaneAPad + j * C::kPlaneB, &maps.wt, ch + 8 * j, co0, 0, &full[st]);
             }
         }
         info[2] = c;
@@ -319,13 +327,15 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const __grid_constant__
                 break;
             }
             tc_fence_after();
-            const uint32_t a0 = smem_u32(stage0 + st * C::kStage), b0 = a0 + 2 * kPlaneAPad;
+            const uint32_t a0 = smem_u32(stage0 + st * C::kStage), b0 = a0 + 2 * C::kPlaneAPad;
 #pragma unroll
-            for (int t = 0; t < 9; t++) {
-                const uint64_t ad = umma_desc(a0 + ((t / 3) * kHaloW + t % 3) * 16, kPlaneAPad, 128);
-                const uint64_t bd = umma_desc(b0 + t * BN * 16, C::kPlaneB, 128);
-                umma_bf16(tmem, ad, bd, idesc, (c | t) != 0);
-            }
+            for (int r = 0; r < R; r++)
+#pragma unroll
+                for (int t = 0; t < 9; t++) {
+                    const uint64_t ad = umma_desc(a0 + ((r + t / 3) * kHaloW + t % 3) * 16, C::kPlaneAPad, 128);
+                    const uint64_t bd = umma_desc(b0 + t * BN * 16, C::kPlaneB, 128);
+                    umma_bf16(tmem + r * BN, ad, bd, idesc, (c | t) != 0);
+                }
             umma_commit(&empty[st]);
         }
         info[3] = c;
@@ -341,12 +351,13 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const __grid_constant__
     } else {
         tc_fence_after();
         const int x = x0 + warp * 32 + lane;
-        const long long p = (long long)row * s.w + x;
 #pragma unroll 1
-        for (int g = 0; g < BN / 16; g++) {
+        for (int q = 0; q < R * (BN / 16); q++) {
+            const int rr = q / (BN / 16), g = q - rr * (BN / 16);
             uint32_t r[16];
-            tmem_ld16(r, tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(g * 16));
-            if (x >= s.w) continue;  // after the warp-wide load
+            tmem_ld16(r, tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(rr * BN + g * 16));
+            if (x >= s.w || y0 + rr >= s.h) continue;  // after the warp-wide load
+            const long long p = ((long long)img * s.h + y0 + rr) * s.w + x;
             const int co = co0 + g * 16;
             uint32_t packed[8];
 #pragma unroll
@@ -668,11 +679,11 @@ static int encode_bf16(CUtensorMap *m, const void *base, int rank, const cuuint6
     return 0;
 }
 
-// Halo map of an NHWC activation: dims (c, w, h, n), box 8 x kHaloW x 3 x 1.
-static int encode_act(CUtensorMap *m, const bf16 *x, int c, const Shape &s) {
+// Halo map of an NHWC activation: dims (c, w, h, n), box 8 x kHaloW x rows x 1.
+static int encode_act(CUtensorMap *m, const bf16 *x, int c, const Shape &s, int rows) {
     const cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)s.w, (cuuint64_t)s.h, (cuuint64_t)s.n};
     const cuuint64_t strides[3] = {(cuuint64_t)c * 2, (cuuint64_t)c * 2 * s.w, (cuuint64_t)c * 2 * s.w * s.h};
-    const cuuint32_t box[4] = {8, (cuuint32_t)kHaloW, 3, 1};
+    const cuuint32_t box[4] = {8, (cuuint32_t)kHaloW, (cuuint32_t)rows, 1};
     return encode_bf16(m, x, 4, dims, strides, box);
 }
 
@@ -687,13 +698,13 @@ static int launch_tc(const TcMaps &maps, int c0, int nck, const float *bias, bf1
             return set_error(FWI_ECUDA, "unet_conv3x3: shared-memory attribute refused");
         attr = true;
     }
-    const int strips = (s.w + kStrip - 1) / kStrip;
-    const long long blocks = (long long)s.n * s.h * strips;
+    const int strips = (s.w + kStrip - 1) / kStrip, groups = (s.h + C::R - 1) / C::R;
+    const long long blocks = (long long)s.n * groups * strips;
     if (blocks >= 0x7fffffffll) return set_error(FWI_ERANGE, "fwi_unet_conv3x3: too many pixel strips");
     const int nst = nck < C::kStages ? nck : C::kStages;
     const size_t smem = kTcHead + 128 + (size_t)nst * C::kStage;
     conv3x3_tc_kernel<BN><<<dim3((unsigned)blocks, cout / BN), 128, smem, st>>>(maps, c0, nck, bias, o0, d0, o1, d1, s,
-                                                                               strips, relu);
+                                                                               strips, groups, relu);
     return check_launch("unet_conv3x3 (tcgen05)");
 }
 
@@ -701,9 +712,11 @@ static int conv3x3_tc(const bf16 *i0, int c0, const bf16 *i1, int c1, const bf16
                       bf16 *o0, int d0, bf16 *o1, int d1, const Shape &s, int relu, cudaStream_t st) {
     const int ct = c0 + c1;
     const int bn = cout % 128 == 0 ? 128 : cout % 64 == 0 ? 64 : cout % 32 == 0 ? 32 : 16;
+    const int rows = (bn >= 128 ? TcConv<128>::R : TcConv<16>::R) + 2;
+    static_assert(TcConv<16>::R == TcConv<32>::R && TcConv<32>::R == TcConv<64>::R, "rows per CTA");
     TcMaps maps;
-    int rc = encode_act(&maps.in0, i0, c0, s);
-    if (!rc) rc = c1 ? encode_act(&maps.in1, i1, c1, s) : encode_act(&maps.in1, i0, c0, s);
+    int rc = encode_act(&maps.in0, i0, c0, s, rows);
+    if (!rc) rc = c1 ? encode_act(&maps.in1, i1, c1, s, rows) : encode_act(&maps.in1, i0, c0, s, rows);
     const cuuint64_t wdims[3] = {(cuuint64_t)ct, (cuuint64_t)cout, 9};
     const cuuint64_t wstr[2] = {(cuuint64_t)ct * 2, (cuuint64_t)ct * 2 * cout};
     const cuuint32_t wbox[3] = {8, (cuuint32_t)bn, 9};
