@@ -271,12 +271,27 @@ class b200:
                 tail = 0.4 * free if self.batch_memory <= 0 else 0.0
                 ea = ExactAdjoint(self.model, nt, self.src_id, lambda s: -1 if combine else chunk[s], n,
                                   self._stf(mode), self.rec_id, tile=self.tile, tail_memory=tail)
+                # the observed traces are stacked into pinned host memory on worker threads while
+                # this thread enqueues the forward sweep, then uploaded on a copy stream that the
+                # misfit waits for
+                staged = [self._stage_pool().submit(self._stack_pinned, slot, [lst[shots.index(i)] for i in chunk])
+                          for slot, (c, lst) in enumerate(data_of)]
                 tr = ea.forward()
                 self.illum_f64 += ea.illum
                 grads = [None, None, None]
-                for c, lst in data_of:
-                    data = torch.from_numpy(np.stack([lst[shots.index(i)] for i in chunk]))
-                    data = data.pin_memory().to(self.device, non_blocking=True)
+                uploads = []
+                for slot, (c, lst) in enumerate(data_of):
+                    host = staged[slot].result()
+                    # allocated from the copy stream's pool, so no block that queued forward work
+                    # still uses can be handed out; recorded on self.stream, which reads it next
+                    with torch.cuda.stream(self._copy_stream()):
+                        data = torch.empty(host.shape, dtype=torch.float32, device=self.device)
+                        data.copy_(host, non_blocking=True)
+                    data.record_stream(self.stream)
+                    uploads.append(data)
+                self.stream.wait_stream(self._copy_stream())
+                for slot, (c, lst) in enumerate(data_of):
+                    data = uploads[slot]
                     grads[c] = torch.empty(n * nrec * nt, dtype=torch.float32, device=self.device)
                     syn = tr[c].reshape(-1).contiguous()
                     misfit += float(engine.misfit_tracegrad(data, syn, grads[c], n, nrec, nt, self.dt).sum().item())
@@ -297,6 +312,31 @@ class b200:
                     self.k_j_f64 -= self.dt * k_buoj * self.dt / torch.where(jj > 0, jj * jj, torch.ones_like(jj))
                 del ea
         return misfit
+
+    def _stage_pool(self):
+        if getattr(self, "_pool", None) is None:
+            from concurrent.futures import ThreadPoolExecutor
+            self._pool = ThreadPoolExecutor(max_workers=3, thread_name_prefix="seispie_b200_stage")
+        return self._pool
+
+    def _copy_stream(self):
+        if getattr(self, "_h2d", None) is None:
+            self._h2d = torch.cuda.Stream(self.device)
+        return self._h2d
+
+    def _stack_pinned(self, slot, arrays):
+        """Stack per-shot trace arrays into pinned host buffer `slot` (kept
+        and grown across calls).  A buffer is rewritten only after the
+        previous call's upload from it has completed: every chunk ends with a
+        host read of its misfit, which follows the upload on the device."""
+        bufs = self.__dict__.setdefault("_pinned", {})
+        n, m = len(arrays), int(np.asarray(arrays[0]).size)
+        buf = bufs.get(slot)
+        if buf is None or buf.numel() < n * m:
+            buf = bufs[slot] = torch.empty(n * m, dtype=torch.float32, pin_memory=True)
+        view = buf[:n * m].view(n, m)
+        np.stack([np.asarray(a).reshape(-1) for a in arrays], out=view.numpy())
+        return view
 
     def _max_batch(self, mode, snapshots):
         budget = self.batch_memory

@@ -214,6 +214,14 @@ def test_plugin_psv_gradient_is_dt_times_exact(tmp_path):
     chi.backward()
     ref = 1e-3 * mu.grad.double().cpu().numpy()
     assert np.linalg.norm(kraw - ref) / np.linalg.norm(ref) < 1e-5
+    # a second call restages the observed traces into the same pinned buffers: same gradient
+    s.compute_gradient()
+    assert np.array_equal(s.k_mu_f64[:, :nz].cpu().numpy(), kraw)
+    # one shot per batch: each batch restages into the buffers the previous one uploaded from
+    s.batch_memory = 1.0
+    s.compute_gradient()
+    k1 = s.k_mu_f64[:, :nz].cpu().numpy()
+    assert np.linalg.norm(k1 - kraw) / np.linalg.norm(kraw) < 1e-6
 
 
 def test_trace_suffix_sum():
