@@ -267,8 +267,7 @@ class b200:
                 # the last steps keep their per-step stores from the forward sweep in part of the free
                 # HBM (those steps are not recomputed; the gradient is the same); not when the
                 # configuration caps the memory of a batch
-                free, _ = torch.cuda.mem_get_info(self.device)
-                tail = 0.4 * free if self.batch_memory <= 0 else 0.0
+                tail = 0.4 * self._free_bytes() if self.batch_memory <= 0 else 0.0
                 ea = ExactAdjoint(self.model, nt, self.src_id, lambda s: -1 if combine else chunk[s], n,
                                   self._stf(mode), self.rec_id, tile=self.tile, tail_memory=tail)
                 # the observed traces are stacked into pinned host memory on worker threads while
@@ -313,6 +312,13 @@ class b200:
                 del ea
         return misfit
 
+    def _free_bytes(self) -> int:
+        """Free device memory including the blocks torch's caching allocator
+        holds unused (those of the previous gradient's buffers), so that
+        every call sizes its buffers alike and reuses the cached blocks."""
+        free, _ = torch.cuda.mem_get_info(self.device)
+        return free + torch.cuda.memory_reserved(self.device) - torch.cuda.memory_allocated(self.device)
+
     def _stage_pool(self):
         if getattr(self, "_pool", None) is None:
             from concurrent.futures import ThreadPoolExecutor
@@ -341,8 +347,7 @@ class b200:
     def _max_batch(self, mode, snapshots):
         budget = self.batch_memory
         if budget <= 0:
-            free, _ = torch.cuda.mem_get_info(self.device)
-            budget = 0.8 * free
+            budget = 0.8 * self._free_bytes()
         return max(1, int(budget // self._shot_bytes(mode, snapshots)))
 
     def _shots(self):
