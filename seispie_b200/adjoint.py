@@ -46,6 +46,19 @@ def default_segment(nt: int, mode: int, nshots: int, grid: Grid, budget_bytes: f
     return min(k, nt)
 
 
+def fixed_bytes(nt: int, mode: int, nshots: int, grid: Grid, nrec: int = 0, segment: int | None = None) -> int:
+    """Upper bound of the device bytes an ExactAdjoint (levels = 1) holds
+    besides its stored tail: checkpoints every K steps over all nt steps, one
+    segment of per-step stores, the forward batch's wavefields (at most two
+    copies of the state) and its traces.  A stored tail has to fit in what
+    is left."""
+    k = segment or default_segment(nt, mode, nshots, grid)
+    field = 4 * nshots * grid.nx * grid.pitch
+    state = NS[mode] + 2 * NV[mode]
+    per_step = strain_fields(mode) + NV[mode]
+    return (math.ceil(nt / k) * state + k * per_step + 2 * state) * field + 3 * 4 * nshots * nrec * nt
+
+
 def two_level_segments(nt: int, mode: int) -> tuple:
     """(K1, K2) minimising the memory of two-level checkpointing,
     nt/K1 + K1/K2 checkpoints of S = NS+2NV fields plus K2 steps of

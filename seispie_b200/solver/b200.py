@@ -257,38 +257,30 @@ class b200:
         """Misfit and exact gradient of this process's shots, accumulated in
         the reference's units (dt * dchi/dparam) into k_lam_f64 / k_mu_f64 /
         k_rho_f64; returns the misfit (sum of per-shot, per-component norms)."""
-        from ..adjoint import ExactAdjoint
+        from ..adjoint import ExactAdjoint, fixed_bytes
         combine = self.config["combine_sources"] == "yes"
         misfit = 0.0
         nrec, nt = self.nrec, self.nt
         for chunk in self._chunks(shots, mode, True):
             n = len(chunk)
             with self._ctx():
-                # the last steps keep their per-step stores from the forward sweep in part of the free
-                # HBM (those steps are not recomputed; the gradient is the same); not when the
-                # configuration caps the memory of a batch
-                tail = 0.4 * self._free_bytes() if self.batch_memory <= 0 else 0.0
+                # the last steps keep their per-step stores from the forward sweep in half of the HBM
+                # that the checkpoints and segment stores leave free (those steps are not recomputed;
+                # the gradient is the same); not when the configuration caps the memory of a batch
+                tail = 0.0
+                if self.batch_memory <= 0:
+                    spare = self._free_bytes() - fixed_bytes(nt, mode, n, self.model.grid, nrec)
+                    tail = 0.5 * max(0.0, spare)
                 ea = ExactAdjoint(self.model, nt, self.src_id, lambda s: -1 if combine else chunk[s], n,
                                   self._stf(mode), self.rec_id, tile=self.tile, tail_memory=tail)
                 # the observed traces are stacked into pinned host memory on worker threads while
                 # this thread enqueues the forward sweep, then uploaded on a copy stream that the
                 # misfit waits for
-                staged = [self._stage_pool().submit(self._stack_pinned, slot, [lst[shots.index(i)] for i in chunk])
-                          for slot, (c, lst) in enumerate(data_of)]
+                staged = self._stage(data_of, chunk, shots)
                 tr = ea.forward()
                 self.illum_f64 += ea.illum
                 grads = [None, None, None]
-                uploads = []
-                for slot, (c, lst) in enumerate(data_of):
-                    host = staged[slot].result()
-                    # allocated from the copy stream's pool, so no block that queued forward work
-                    # still uses can be handed out; recorded on self.stream, which reads it next
-                    with torch.cuda.stream(self._copy_stream()):
-                        data = torch.empty(host.shape, dtype=torch.float32, device=self.device)
-                        data.copy_(host, non_blocking=True)
-                    data.record_stream(self.stream)
-                    uploads.append(data)
-                self.stream.wait_stream(self._copy_stream())
+                uploads = self._upload(staged)
                 for slot, (c, lst) in enumerate(data_of):
                     data = uploads[slot]
                     grads[c] = torch.empty(n * nrec * nt, dtype=torch.float32, device=self.device)
@@ -318,6 +310,28 @@ class b200:
         every call sizes its buffers alike and reuses the cached blocks."""
         free, _ = torch.cuda.mem_get_info(self.device)
         return free + torch.cuda.memory_reserved(self.device) - torch.cuda.memory_allocated(self.device)
+
+    def _stage(self, data_of, chunk, shots):
+        """Start stacking the observed traces of `chunk` into the pinned
+        buffers (one per component slot) on worker threads."""
+        return [self._stage_pool().submit(self._stack_pinned, slot, [lst[shots.index(i)] for i in chunk])
+                for slot, (c, lst) in enumerate(data_of)]
+
+    def _upload(self, staged):
+        """Upload the staged traces on the copy stream; self.stream waits for
+        them.  Returns the device tensors, one per component slot."""
+        out = []
+        for f in staged:
+            host = f.result()
+            # allocated from the copy stream's pool, so no block that queued forward work still
+            # uses can be handed out; recorded on self.stream, which reads it next
+            with torch.cuda.stream(self._copy_stream()):
+                data = torch.empty(host.shape, dtype=torch.float32, device=self.device)
+                data.copy_(host, non_blocking=True)
+            data.record_stream(self.stream)
+            out.append(data)
+        self.stream.wait_stream(self._copy_stream())
+        return out
 
     def _stage_pool(self):
         if getattr(self, "_pool", None) is None:
@@ -531,13 +545,14 @@ class b200:
                 misfit += self._exact_gradient(mode, shots, data_of[mode])
                 continue
             for chunk in self._chunks(shots, mode, adj):
+                staged = self._stage(data_of[mode], chunk, shots)  # on worker threads during the forward
                 b = self._forward_batch(mode, chunk, snapshots=bool(adj), snap_velocity=snapv)
                 n, nrec, nt = len(chunk), self.nrec, self.nt
                 with self._ctx():
                     adstf = [None, None, None]
-                    for c, lst in data_of[mode]:
-                        data = torch.from_numpy(np.stack([lst[shots.index(i)] for i in chunk]))
-                        data = data.pin_memory().to(self.device, non_blocking=True)
+                    uploads = self._upload(staged)
+                    for slot, (c, lst) in enumerate(data_of[mode]):
+                        data = uploads[slot]
                         adstf[c] = torch.empty(n * nrec * nt, dtype=torch.float32, device=self.device)
                         m = engine.misfit(data, b.obs[c], adstf[c], n, nrec, nt, self.dt)
                         misfit += float(m.sum().item())

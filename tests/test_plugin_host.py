@@ -111,3 +111,22 @@ def test_setup_refuses_without_cuda():
     s.path, s.mpi = {}, None
     with pytest.raises(RuntimeError, match="CUDA"):
         s.setup(None)
+
+
+def test_exact_adjoint_fixed_bytes():
+    """The memory bound the plugin sizes its stored tail against: checkpoints
+    every K steps over all nt steps, K steps of per-step stores, two copies
+    of the state and the traces, all of nshots shots."""
+    from seispie_b200._lib import FWI_PSV, FWI_SPIN
+    from seispie_b200.adjoint import default_segment, fixed_bytes
+    from seispie_b200.engine import Grid
+    g = Grid(1024, 510, 10.0, 10.0)  # pitch 512
+    field = 4 * 64 * 1024 * 512
+    k = default_segment(6000, FWI_PSV, 64, g)
+    assert k == 92
+    want = (66 * 7 + 92 * 5 + 2 * 7) * field + 3 * 4 * 64 * 256 * 6000
+    assert fixed_bytes(6000, FWI_PSV, 64, g, 256) == want
+    # an explicit segment; the spin state is 6 stress + 2 x 3 velocity/displacement fields,
+    # and a step stores 6 strain terms and 3 divergences
+    assert fixed_bytes(100, FWI_SPIN, 2, Grid(8, 8, 1.0, 1.0), 0, segment=10) == \
+        (10 * 12 + 10 * 9 + 2 * 12) * 4 * 2 * 8 * 8
