@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define FWI_ABI_VERSION 4
+#define FWI_ABI_VERSION 5
 
 /* status codes */
 #define FWI_OK 0
@@ -52,7 +52,8 @@ extern "C" {
  *              spin adds {syx_c, syy_c, syz_c} in slots 3..5
  *   vel[2][3]  velocity, ping-pong pair; SH: {vy}; P-SV: {vx, vz};
  *              spin adds vy_c in slot 2
- *   disp[3]    displacement, updated in place, same slots as vel
+ *   disp[3]    displacement, updated in place, same slots as vel; all NULL
+ *              for a displacement-free batch (fwi_run)
  * `cur` selects which half of each pair holds the current state; fwi_run
  * flips it once per step.
  * Model (shared by all shots, [nx][pitch]; prepared by fwi_prepare_model):
@@ -113,10 +114,20 @@ typedef struct fwi_batch {
     /* Spin gradients of fwi_run_transposed (FP64 [nx][pitch], NULL skips):
      * dL/dnu, dL/d(mu_c+nu_c), dL/d(dt/j). */
     double *k_nu, *k_mnc, *k_buoj;
+    /* Receivers listed by cell: a permutation of 0 .. nrec-1 with
+     * rec_cell[rec_order[i]] non-decreasing.  Required by displacement-free
+     * forward runs that record traces (see fwi_run). */
+    const int *rec_order;
 } fwi_batch;
 
 /* ABI version of the loaded library (FWI_ABI_VERSION). */
 int fwi_abi_version(void);
+
+/* Binary version (major*10 + minor) of the device code the library runs on
+ * the current device, from cudaFuncGetAttributes: 100 for sm_100a.  A
+ * negative FWI_ECUDA code without a usable device.  No counterpart in the
+ * reference. */
+int fwi_binary_version(void);
 
 /* Number of kernels this library has launched in the process so far (for
  * launch accounting by benchmarks).  No counterpart in the reference. */
@@ -183,7 +194,16 @@ int fwi_prepare_model(const float *rho, const float *j, const float *mu_c, const
  *   (same step with the adjoint source, plus the interaction kernels every
  *   sae steps with ndt = sae*dt).  Requires the forward snapshots.
  * The caller clears the wavefields first (fwi_clear or cudaMemsetAsync),
- * as clear_wavefields does (fd2d.py:318-341).  b->cur is updated. */
+ * as clear_wavefields does (fd2d.py:318-341).  b->cur is updated.
+ * Displacement-free batches (disp[] all NULL; SH or P-SV forward, nz <= 1024,
+ * no snapshots): the displacement, which the reference keeps as a field only
+ * to feed save_obs, is not stored.  The step runs on the row-marching kernel
+ * and each recorded trace is the running sum u(it) = u(it-1) + v(it) dt of
+ * the velocity at its receiver, evaluated in the same float operations as
+ * add_vy / add_vxz (solver.py:95-109), so the traces are bit-identical to a
+ * run with displacement fields.  Such batches need rec_order when they
+ * record, and the injection entries of each shot sorted by cell (entries at
+ * one cell keep their relative order, which fixes their summation order). */
 int fwi_run(fwi_batch *b, int adjoint, int it0, int nsteps, void *stream);
 
 /* Uneven batches: n independent forward batches of one mode (each with its
@@ -273,8 +293,9 @@ int fwi_axpby(float *out, double a, const float *x, double b, const float *y, lo
  * same arguments and results as fwi_misfit minus `partial`, whose role is
  * taken by a fixed array inside the library (FWI_MISFIT_NOALLOC_MAX_PARTIALS
  * doubles on every device that loads the library, until exit).  Larger
- * batches are rejected with FWI_ERANGE.  The first call on a device looks up
- * the array's address (that device current); make it outside stream capture.
+ * batches are rejected with FWI_ERANGE.  Each call looks up the array's
+ * address on the current device; the first call on a device may load the
+ * library's device code there, so make it outside stream capture.
  * All calls share the array: calls that overlap on the GPU race, so keep them
  * in order on one stream.  It allocates nothing.  No counterpart in the
  * reference. */

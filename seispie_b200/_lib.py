@@ -13,7 +13,7 @@ from . import build as _build
 
 FWI_SH, FWI_PSV, FWI_SPIN = 0, 1, 2
 MODES = {"sh": FWI_SH, "psv": FWI_PSV, "spin": FWI_SPIN}
-ABI_VERSION = 4
+ABI_VERSION = 5
 
 _fp = ctypes.POINTER(ctypes.c_float)
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -34,7 +34,7 @@ class FwiBatch(ctypes.Structure):
         ("sae", ctypes.c_int), ("nsa", ctypes.c_int), ("snap_u", _vp * 3), ("snap_v", _vp * 3),
         ("k_lam", _vp), ("k_mu", _vp), ("k_rho", _vp),
         ("seg_e", _vp * 6), ("seg_ds", _vp * 3), ("seg0", ctypes.c_int), ("nseg", ctypes.c_int),
-        ("k_nu", _vp), ("k_mnc", _vp), ("k_buoj", _vp),
+        ("k_nu", _vp), ("k_mnc", _vp), ("k_buoj", _vp), ("rec_order", _vp),
     ]
 
 
@@ -63,6 +63,7 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     sigs = {
         "fwi_abi_version": ([], ctypes.c_int),
         "fwi_launch_count": ([], ctypes.c_longlong),
+        "fwi_binary_version": ([], ctypes.c_int),
         "fwi_last_error": ([ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
         "fwi_device_status": ([ctypes.POINTER(ctypes.c_int), ctypes.c_int], ctypes.c_int),
         "fwi_unet_conv_path": ([ctypes.c_int], ctypes.c_int),

@@ -33,10 +33,17 @@ def strain_fields(mode: int) -> int:
     return 2 if mode == FWI_SH else 3 if mode == FWI_PSV else 6
 
 
+def state_fields(mode: int, grid: Grid) -> int:
+    """Fields of one checkpoint: stress and velocity, plus the displacement
+    where the forward keeps it (engine.displacement_free_ok)."""
+    return NS[mode] + (1 if engine.displacement_free_ok(mode, grid) else 2) * NV[mode]
+
+
 def default_segment(nt: int, mode: int, nshots: int, grid: Grid, budget_bytes: float | None = None) -> int:
     """Segment length K minimising checkpoint + segment memory
-    (nt/K * (NS+2NV) fields + K * (NE+NV) fields), then shrunk to the budget."""
-    state = NS[mode] + 2 * NV[mode]
+    (nt/K * S fields + K * (NE+NV) fields, S = state_fields), then shrunk to
+    the budget."""
+    state = state_fields(mode, grid)
     per_step = strain_fields(mode) + NV[mode]
     k = max(1, int(round(math.sqrt(nt * state / per_step))))
     if budget_bytes:
@@ -49,14 +56,16 @@ def default_segment(nt: int, mode: int, nshots: int, grid: Grid, budget_bytes: f
 def fixed_bytes(nt: int, mode: int, nshots: int, grid: Grid, nrec: int = 0, segment: int | None = None) -> int:
     """Upper bound of the device bytes an ExactAdjoint (levels = 1) holds
     besides its stored tail: checkpoints every K steps over all nt steps, one
-    segment of per-step stores, the forward batch's wavefields (at most two
-    copies of the state) and its traces.  A stored tail has to fit in what
-    is left."""
+    segment of per-step stores, the wavefields of the forward and adjoint
+    batches (ping-pong stress and velocity, displacement where kept) and, per
+    velocity component, the traces, the observed data and the trace
+    gradients.  A stored tail has to fit in what is left."""
     k = segment or default_segment(nt, mode, nshots, grid)
     field = 4 * nshots * grid.nx * grid.pitch
-    state = NS[mode] + 2 * NV[mode]
+    state = state_fields(mode, grid)
     per_step = strain_fields(mode) + NV[mode]
-    return (math.ceil(nt / k) * state + k * per_step + 2 * state) * field + 3 * 4 * nshots * nrec * nt
+    batch = 2 * NS[mode] + 2 * NV[mode] + (state - NS[mode] - NV[mode])
+    return (math.ceil(nt / k) * state + k * per_step + 2 * batch) * field + 3 * 4 * nshots * nrec * nt * NV[mode]
 
 
 def two_level_segments(nt: int, mode: int) -> tuple:
@@ -111,7 +120,10 @@ class ExactAdjoint:
         self.t0 = self.nt - self.tail  # steps [t0, nt) keep their stores from the forward sweep
         self.nseg = math.ceil(self.t0 / self.K)
         self.fwd = ShotBatch(model, self.nshots, self.nt, self.rec_id, tile=tile)
-        self.fdesc = self.fwd.desc(inj=injection_lists(self.nshots, src_id, isrc_of_shot), stf=stf)
+        inj = injection_lists(self.nshots, src_id, isrc_of_shot)
+        self.fdesc = self.fwd.desc(inj=inj, stf=stf)
+        # recomputed steps record no traces (the forward sweep has them)
+        self.rdesc = self.fwd.desc(inj=inj, stf=stf, record=False)
         dev = model.device
         shape = (self.nshots, g.nx, g.pitch)
         nstate = len(self.fwd.state_tensors())
@@ -149,11 +161,17 @@ class ExactAdjoint:
             n = min(self.K, self.t0 - s * self.K)
             b.run(self.fdesc, False, s * self.K, n)
         if self.tail:
+            # the illumination is sampled at the multiples of K whatever the tail, so that it does not
+            # depend on how much memory the tail got
             b.set_segment(self.fdesc, self.tail_e, self.tail_ds, self.t0, self.tail)
-            for s0 in range(self.t0, self.nt, self.K):
-                for v in b.vel[b.cur]:
-                    engine.energy_accumulate(v, self.illum)
-                b.run(self.fdesc, False, s0, min(self.K, self.nt - s0))
+            s0 = self.t0
+            while s0 < self.nt:
+                if s0 % self.K == 0:
+                    for v in b.vel[b.cur]:
+                        engine.energy_accumulate(v, self.illum)
+                s1 = min(self.nt, (s0 // self.K + 1) * self.K)
+                b.run(self.fdesc, False, s0, s1 - s0)
+                s0 = s1
             b.set_segment(self.fdesc, [None] * 6, [None] * 3, 0, 0)
         return [b.traces(c).clone() if b.obs[c] is not None else None for c in range(3)]
 
@@ -184,8 +202,8 @@ class ExactAdjoint:
         def reverse(t0, n):
             """Recompute steps [t0, t0+n) from the current state with the
             per-step stores and run their transposes."""
-            fwd.set_segment(self.fdesc, self.seg_e, self.seg_ds, t0, n)
-            fwd.run(self.fdesc, False, t0, n)
+            fwd.set_segment(self.rdesc, self.seg_e, self.seg_ds, t0, n)
+            fwd.run(self.rdesc, False, t0, n)
             adj.set_segment(adesc, self.seg_e, self.seg_ds, t0, n)
             adj.run_transposed(adesc, t0 + n, n)
 
@@ -200,17 +218,17 @@ class ExactAdjoint:
                 reverse(s0, n)
                 continue
             nsub = math.ceil(n / self.K2)
-            fwd.set_segment(self.fdesc, [None] * 6, [None] * 3, 0, 0)
+            fwd.set_segment(self.rdesc, [None] * 6, [None] * 3, 0, 0)
             for jj in range(nsub):  # sub-checkpoints of this segment
                 for q, t in enumerate(fwd.state_tensors()):
                     self.ckpt2[jj, q].copy_(t)
                 if jj < nsub - 1:
-                    fwd.run(self.fdesc, False, s0 + jj * self.K2, self.K2)
+                    fwd.run(self.rdesc, False, s0 + jj * self.K2, self.K2)
             for jj in reversed(range(nsub)):
                 for q, t in enumerate(fwd.state_tensors()):
                     t.copy_(self.ckpt2[jj, q])
                 reverse(s0 + jj * self.K2, min(self.K2, n - jj * self.K2))
-        fwd.set_segment(self.fdesc, [None] * 6, [None] * 3, 0, 0)
+        fwd.set_segment(self.rdesc, [None] * 6, [None] * 3, 0, 0)
         return tuple(k)
 
 

@@ -25,7 +25,7 @@ def autotune(model: DeviceModel, nshots: int, nt: int, rec_id, inj, stf, steps: 
     steps = max(1, min(steps, nt - warm))
     times: dict[int, float] = {}
     for t in variants or _lib.tile_variants():
-        b = ShotBatch(model, nshots, nt, rec_id, tile=t)
+        b = ShotBatch(model, nshots, nt, rec_id, tile=t, displacement=True)
         d = b.desc(inj=inj, stf=stf)
         b.clear()
         b.run(d, False, 0, min(warm, nt))

@@ -10,6 +10,7 @@ PyTorch, so device pointers and streams from torch can be passed to it.
 from __future__ import annotations
 
 import argparse
+import json
 import os
 import subprocess
 import sys
@@ -19,7 +20,8 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 OUT_DIR = os.path.join(PKG, "_build")
 LIB = os.path.join(OUT_DIR, "libseispie_b200.so")
-SOURCES = ("capi.cu", "step.cu", "aux.cu", "linalg.cu", "noalloc.cu", "unet.cu")
+INFO = os.path.join(OUT_DIR, "build_info.json")
+SOURCES = ("capi.cu", "step.cu", "march.cu", "aux.cu", "linalg.cu", "noalloc.cu", "unet.cu")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -43,13 +45,14 @@ def build(verbose: bool = False, force: bool = False) -> str:
     Skips the work when the library is newer than every source."""
     os.makedirs(OUT_DIR, exist_ok=True)
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    deps = srcs + [os.path.join(CSRC, "common.cuh"), os.path.join(ROOT, "include", "seispie_b200.h")]
+    deps = srcs + [os.path.join(CSRC, h) for h in ("common.cuh", "stencil.cuh")] + [os.path.join(ROOT, "include", "seispie_b200.h")]
     if not force and os.path.exists(LIB) and all(os.path.getmtime(LIB) >= os.path.getmtime(d) for d in deps):
         return LIB
-    objs = []
+    objs, cmds = [], []
     for s in srcs:
         o = os.path.join(OUT_DIR, os.path.basename(s) + ".o")
         cmd = [nvcc(), "-c", s, "-o", o] + flags(verbose)
+        cmds.append(cmd)
         r = subprocess.run(cmd, capture_output=True, text=True)
         if verbose or r.returncode:
             sys.stderr.write(r.stdout + r.stderr)
@@ -63,6 +66,10 @@ def build(verbose: bool = False, force: bool = False) -> str:
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("link failed")
     os.replace(tmp, LIB)
+    # the exact commands, for checks of the target architecture without inspecting the binary
+    with open(INFO, "w") as f:
+        json.dump({"compile": [" ".join(c) for c in cmds], "link": " ".join(cmd), "arch": " ".join(ARCH)}, f,
+                  indent=1)
     return LIB
 
 

@@ -36,6 +36,10 @@ int launch_step(const fwi_batch *b, int adjoint, int it, bool snap_u_next, int s
                 int snap_v_slot, cudaStream_t st);
 int launch_interaction(const fwi_batch *b, int isae, cudaStream_t st);
 int launch_adjoint_step(const fwi_batch *b, int it, cudaStream_t st);
+int launch_march(const fwi_batch *b, int it, cudaStream_t st);
+bool march_supported(const fwi_batch *b);
+int launch_displacement_traces(float *obs, long long ntr, int nt, int it0, int n, double dt, cudaStream_t st);
+int kernel_binary_version(int *v);
 long long multi_workspace_bytes(int n);
 int multi_prepare(fwi_batch *const *bs, int n, void *ws, int (*check)(const fwi_batch *, int, int, int));
 int multi_run(fwi_batch *const *bs, int n, void *ws, int it0, int nsteps, cudaStream_t st);
@@ -86,7 +90,10 @@ static int check_batch(const fwi_batch *b, int adjoint, int it0, int nsteps) {
         for (int q = 0; q < nv; q++)
             REQUIRE(b->vel[h][q] && aligned16(b->vel[h][q]), "vel[%d][%d] NULL or not 16-byte aligned", h, q);
     }
-    for (int q = 0; q < nv; q++) REQUIRE(b->disp[q] && aligned16(b->disp[q]), "disp[%d] NULL or misaligned", q);
+    const bool nodisp = !b->disp[0];
+    for (int q = 0; q < nv; q++)
+        REQUIRE(nodisp ? !b->disp[q] : (b->disp[q] && aligned16(b->disp[q])),
+                "disp[] must be all NULL (displacement-free) or all set and 16-byte aligned (disp[%d])", q);
     REQUIRE(b->buo && b->bound && b->mu && aligned16(b->buo) && aligned16(b->bound) && aligned16(b->mu),
             "buo, bound and mu must be non-NULL and 16-byte aligned");
     if (b->mode != FWI_SH) REQUIRE(b->lam && aligned16(b->lam), "lam must be non-NULL and 16-byte aligned");
@@ -99,6 +106,15 @@ static int check_batch(const fwi_batch *b, int adjoint, int it0, int nsteps) {
         else REQUIRE(b->stf[0] && b->stf[2], "P-SV injection needs stf[0] and stf[2]");
     }
     if (b->nrec > 0 && !adjoint) REQUIRE(b->rec_cell, "rec_cell is required when nrec > 0");
+    if (nodisp && nsteps > 0) {
+        REQUIRE(!adjoint, "the continuous adjoint (adjoint = 1) needs displacement fields");
+        REQUIRE(march_supported(b), "displacement-free batches: SH or P-SV with nz <= 1024 (mode %d, nz %d)", b->mode,
+                b->nz);
+        for (int c = 0; c < 3; c++)
+            REQUIRE(!b->snap_u[c] && !b->snap_v[c], "displacement-free batches take no snapshots");
+        const bool rec = b->nrec > 0 && (b->obs[0] || b->obs[1] || b->obs[2]);
+        REQUIRE(!rec || b->rec_order, "displacement-free batches that record traces need rec_order");
+    }
     if (adjoint) {
         REQUIRE(b->sae >= 1, "the adjoint needs adjoint_interval >= 1");
         REQUIRE(b->nsa >= 1, "the adjoint needs nsa >= 1 snapshots");
@@ -127,13 +143,20 @@ int fwi_abi_version(void) { return FWI_ABI_VERSION; }
 
 long long fwi_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
+int fwi_binary_version(void) {
+    int v = 0;
+    const int rc = kernel_binary_version(&v);
+    return rc ? rc : v;
+}
+
 int fwi_device_status(int *status, int clear) {
     if (!status) return set_error(FWI_EINVAL, "fwi_device_status: NULL status");
-    int a = 0, b = 0;
+    int a = 0, m = 0, b = 0;
     int rc = step_device_status(clear, &a);
+    if (!rc) rc = march_device_status(clear, &m);
     if (!rc) rc = unet_device_status(clear, &b);
     if (rc) return rc;
-    *status = (a ? 1 : 0) | (b ? 2 : 0);
+    *status = (a || m ? 1 : 0) | (b ? 2 : 0);
     return 0;
 }
 
@@ -196,6 +219,22 @@ int fwi_run(fwi_batch *b, int adjoint, int it0, int nsteps, void *stream) {
     int rc = check_batch(b, adjoint, it0, nsteps);
     if (rc) return rc;
     cudaStream_t st = (cudaStream_t)stream;
+    if (!b->disp[0]) {
+        // displacement-free: row-marching steps recording velocity at the
+        // receivers, then the traces' running sums over these steps
+        for (int it = it0; it < it0 + nsteps; it++) {
+            rc = launch_march(b, it, st);
+            if (rc) return rc;
+            b->cur ^= 1;
+        }
+        const long long ntr = (long long)b->nshots * b->nrec;
+        for (int c = 0; c < 3 && b->nrec > 0; c++) {
+            if (!b->obs[c]) continue;
+            rc = launch_displacement_traces(b->obs[c], ntr, b->nt, it0, nsteps, b->dt, st);
+            if (rc) return rc;
+        }
+        return 0;
+    }
     const long long field = (long long)b->nshots * b->nx * b->pitch;
     const int sae = b->sae, nsa = b->nsa;
     if (!adjoint && sae > 0 && nsteps > 0 && (it0 + 1) % sae == 0) {

@@ -88,6 +88,17 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
         : "memory");
 }
 
+// Untiled bulk copy global -> shared of `bytes` bytes (both addresses 16-byte
+// aligned, bytes a multiple of 16), completion counted on `bar`.  No
+// multicast: the source may be any global memory.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
 // cuTensorMapEncodeTiled, fetched from the driver at run time.
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
@@ -115,6 +126,7 @@ int check_launch(const char *what);
 // Device-side status words of the kernels with bounded waits, read (and
 // optionally cleared) by fwi_device_status; each source file owns its own.
 int step_device_status(int clear, int *status);
+int march_device_status(int clear, int *status);
 int unet_device_status(int clear, int *status);
 
 }  // namespace fwi

@@ -10,15 +10,15 @@
 // array inside the library (FWI_MISFIT_NOALLOC_MAX_PARTIALS doubles, 1 MiB,
 // held on every device that loads the library until the process exits).
 //
-// Set-up: the first call on a device (that device current) looks up the
-// array's device address with cudaGetSymbolAddress and caches it; make that
-// first call outside any stream capture.  The array is shared by every call:
+// Set-up: every call looks up the array's device address on the current
+// device with cudaGetSymbolAddress (cheap, allocates nothing), so the address
+// is never stale, also after cudaDeviceReset.  The first call on a device may
+// load the library's device code there; make it before any stream capture.
+// The array is shared by every call:
 // calls whose work overlaps on the GPU (other streams, other host threads)
 // race on it, so issue them in order on one stream.  It keeps the last call's
 // partial sums; nothing needs clearing, because every call writes each partial
 // sum before its final reduction reads it.
-#include <mutex>
-
 #include "common.cuh"
 
 namespace fwi {
@@ -29,26 +29,15 @@ long long misfit_partials(int nrec, int nt);
 
 static __device__ __align__(256) double g_misfit_scratch[FWI_MISFIT_NOALLOC_MAX_PARTIALS];
 
-constexpr int kMaxDevices = 64;
-static std::mutex g_scratch_mu;
-static double *g_scratch_ptr[kMaxDevices] = {};
-
-// Device address of g_misfit_scratch on the current device (looked up once
-// per device).  In host code the array's name only stands in for the symbol.
+// Device address of g_misfit_scratch on the current device, looked up on
+// every call.  In host code the array's name only stands in for the symbol;
+// a kernel given it directly would read host memory or fault.
 static int misfit_scratch(double **out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return set_error(FWI_ECUDA, "fwi_misfit_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
-    if (dev < 0 || dev >= kMaxDevices) return set_error(FWI_ERANGE, "fwi_misfit_noalloc: device %d >= %d", dev, kMaxDevices);
-    std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_ptr[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_misfit_scratch);
-        if (e != cudaSuccess)
-            return set_error(FWI_ECUDA, "fwi_misfit_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
-        g_scratch_ptr[dev] = static_cast<double *>(p);
-    }
-    *out = g_scratch_ptr[dev];
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_misfit_scratch);
+    if (e != cudaSuccess)
+        return set_error(FWI_ECUDA, "fwi_misfit_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+    *out = static_cast<double *>(p);
     return 0;
 }
 

@@ -42,34 +42,11 @@
 #include <cstdio>
 
 #include "common.cuh"
+#include "stencil.cuh"
 
 namespace cg = cooperative_groups;
 
 namespace fwi {
-
-template <int MODE>
-struct Fields;
-// NS stress fields (with halo), NV velocity/displacement components,
-// NVP per-cell parameters of the velocity half, NIP of the stress half,
-// NINJ injected components.
-template <>
-struct Fields<FWI_SH> {
-    static constexpr int NS = 2, NV = 1, NVP = 2, NIP = 1, NINJ = 1;
-};
-template <>
-struct Fields<FWI_PSV> {
-    static constexpr int NS = 3, NV = 2, NVP = 2, NIP = 2, NINJ = 2;
-};
-template <>
-struct Fields<FWI_SPIN> {
-    static constexpr int NS = 6, NV = 3, NVP = 3, NIP = 4, NINJ = 2;
-};
-
-// Stress fields whose D_x^- is taken (SH: sxy; P-SV: sxx, sxz; spin also
-// syx_c, syy_c) -- these get an x register window in step_kernel_rw.
-__host__ __device__ constexpr bool takes_dxm(int mode, int f) {
-    return mode == FWI_SH ? f == 0 : (f == 0 || f == 2 || (mode == FWI_SPIN && (f == 3 || f == 4)));
-}
 
 struct StepArgs {
     int nx, nz, pitch, nt, it, nrec;
@@ -955,6 +932,7 @@ int multi_prepare(fwi_batch *const *bs, int n, void *ws, int (*check)(const fwi_
         if (bs[i]->mode != mode || bs[i]->tile != bs[0]->tile)
             return set_error(FWI_EINVAL, "fwi_multi_prepare: all batches need the same mode and tile");
         if (bs[i]->cur != bs[0]->cur) return set_error(FWI_EINVAL, "fwi_multi_prepare: batches out of step (cur)");
+        if (!bs[i]->disp[0]) return set_error(FWI_EINVAL, "fwi_multi_prepare: batches need displacement fields");
     }
     int *order = new int[n];
     long long *prefix = new long long[n + 1];

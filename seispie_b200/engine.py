@@ -140,6 +140,16 @@ def point_ids(points: np.ndarray, dx, dz, nz: int) -> np.ndarray:
     return ids
 
 
+# widest grid (z cells) the row-marching step kernel of displacement-free batches takes
+MARCH_MAX_NZ = 1024
+
+
+def displacement_free_ok(mode: int, grid: Grid, snapshots: bool = False) -> bool:
+    """Whether a forward batch can run without displacement fields (the
+    row-marching step kernel): SH or P-SV, nz <= 1024, no snapshots."""
+    return mode in (FWI_SH, FWI_PSV) and grid.nz <= MARCH_MAX_NZ and not snapshots
+
+
 class ShotBatch:
     """State of ``nshots`` concurrent shots on one model: ping-pong stress and
     velocity pairs, displacement, receiver traces and (optionally) the
@@ -147,23 +157,38 @@ class ShotBatch:
 
     ``inj``: (ptr[nshots+1], cell[], row[]) int32 host arrays; entry e of shot
     s adds stf[row[e]*nt + it] at cell[e] (reference cell numbering).
+
+    ``displacement``: keep displacement fields (True), or not (False: the
+    traces are rebuilt from the velocity at the receivers, bit-identically,
+    and the step runs on the row-marching kernel); None picks False wherever
+    that kernel applies (``displacement_free_ok``).  ``tile`` selects the
+    tiled kernel variant of batches with displacement fields.
     """
 
     def __init__(self, model: DeviceModel, nshots: int, nt: int, rec_cell: np.ndarray, sae: int = 0,
-                 nsa: int = 0, snapshots: bool = False, snap_velocity: bool = False, tile: int = 0):
+                 nsa: int = 0, snapshots: bool = False, snap_velocity: bool = False, tile: int = 0,
+                 displacement: bool | None = None):
         self.model, self.grid, self.mode = model, model.grid, model.mode
         self.nshots, self.nt, self.sae, self.nsa = int(nshots), int(nt), int(sae), int(nsa)
         self.device, self.stream = model.device, model.stream
         g = self.grid
+        if displacement is None:
+            displacement = not displacement_free_ok(self.mode, g, snapshots)
+        elif not displacement and not displacement_free_ok(self.mode, g, snapshots):
+            raise ValueError("a displacement-free batch needs SH or P-SV, nz <= %d and no snapshots" % MARCH_MAX_NZ)
+        self.has_disp = bool(displacement)
         shape = (self.nshots, g.nx, g.pitch)
         ns, nv = NS[self.mode], NV[self.mode]
         z = lambda *s: torch.zeros(s, dtype=torch.float32, device=self.device)  # noqa: E731
         with torch.cuda.stream(self.stream) if self.stream is not None else _null():
             self.sig = [[z(*shape) for _ in range(ns)] for _ in range(2)]
             self.vel = [[z(*shape) for _ in range(nv)] for _ in range(2)]
-            self.disp = [z(*shape) for _ in range(nv)]
+            self.disp = [z(*shape) for _ in range(nv)] if self.has_disp else []
             self.nrec = len(rec_cell)
-            self.rec_cell = torch.as_tensor(np.asarray(rec_cell, dtype=np.int32)).to(self.device)
+            rc = np.asarray(rec_cell, dtype=np.int32)
+            self.rec_cell = torch.as_tensor(rc).to(self.device)
+            # receivers by cell (stable), for the row-marching kernel's walk
+            self.rec_order = torch.as_tensor(np.argsort(rc, kind="stable").astype(np.int32)).to(self.device)
             self.obs = [None, None, None]
             for q in range(nv):
                 self.obs[COMP[self.mode][q]] = z(self.nshots * max(self.nrec, 1) * self.nt)
@@ -207,6 +232,7 @@ class ShotBatch:
                 b.stf[c] = ptr(stf[c])
         b.nrec = self.nrec
         b.rec_cell = ptr(self.rec_cell) if self.nrec else None
+        b.rec_order = ptr(self.rec_order) if self.nrec else None
         for c in range(3):
             b.obs[c] = ptr(self.obs[c]) if record else None
             b.snap_u[c] = ptr(self.snap_u[c])
@@ -265,6 +291,8 @@ class ShotBatch:
         if name in v_names:
             return self.vel[self.cur][v_names.index(name)][:, :, :nz]
         if name in u_names:
+            if not self.has_disp:
+                raise KeyError("%s: this batch keeps no displacement fields (displacement=False)" % name)
             return self.disp[u_names.index(name)][:, :, :nz]
         raise KeyError(name)
 
@@ -273,10 +301,23 @@ class ShotBatch:
         return self.obs[comp].view(self.nshots, max(self.nrec, 1), self.nt)[:, : self.nrec]
 
 
+def _sort_by_cell(ptr_: np.ndarray, cell: np.ndarray, row: np.ndarray) -> tuple:
+    """Entries of every shot ordered by cell, stably: entries at one cell
+    keep their order, so each cell's sum (taken in entry order) is
+    unchanged; the row-marching step kernel visits them in this order."""
+    for s in range(len(ptr_) - 1):
+        lo, hi = int(ptr_[s]), int(ptr_[s + 1])
+        o = np.argsort(cell[lo:hi], kind="stable")
+        cell[lo:hi] = cell[lo:hi][o]
+        row[lo:hi] = row[lo:hi][o]
+    return ptr_, cell, row
+
+
 def injection_lists(nshots: int, src_id: np.ndarray, isrc_of_shot) -> tuple:
     """CSR injection lists for a forward batch.  isrc_of_shot(s) returns -1
     for 'all sources' (combine_sources = yes) or the one source index of shot
-    s (solver.py:180-183, stf_dsy's isrc test at solver.py:81)."""
+    s (solver.py:180-183, stf_dsy's isrc test at solver.py:81).  The entries
+    of a shot are ordered by cell, sources on one cell in source order."""
     ptr_, cell, row = [0], [], []
     for s in range(nshots):
         isrc = isrc_of_shot(s)
@@ -285,17 +326,18 @@ def injection_lists(nshots: int, src_id: np.ndarray, isrc_of_shot) -> tuple:
             cell.append(int(src_id[i]))
             row.append(int(i))
         ptr_.append(len(cell))
-    return (np.asarray(ptr_, np.int32), np.asarray(cell, np.int32), np.asarray(row, np.int32))
+    return _sort_by_cell(np.asarray(ptr_, np.int32), np.asarray(cell, np.int32), np.asarray(row, np.int32))
 
 
 def adjoint_injection_lists(nshots: int, rec_id: np.ndarray) -> tuple:
     """Adjoint sources: every receiver of every shot, row = shot*nrec + r
-    (solver.py:311: stf_dsy over rec_id with isrc = -1)."""
+    (solver.py:311: stf_dsy over rec_id with isrc = -1), ordered by cell
+    within a shot (receivers on one cell in receiver order)."""
     nrec = len(rec_id)
     ptr_ = np.arange(nshots + 1, dtype=np.int32) * nrec
     cell = np.tile(np.asarray(rec_id, np.int32), nshots)
     row = np.arange(nshots * nrec, dtype=np.int32)
-    return ptr_, cell, row
+    return _sort_by_cell(ptr_, cell, row)
 
 
 def ricker_stf(src: np.ndarray, nt: int, dt: float, device, stream=None):

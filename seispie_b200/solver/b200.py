@@ -231,12 +231,11 @@ class b200:
         g = self.grid
         field = g.nx * g.pitch * 4
         ns, nv = engine.NS[mode], engine.NV[mode]
-        b = (2 * ns + 3 * nv) * field + 4 * self.nrec * self.nt * nv * 3
         if snapshots and self._exact(mode):
-            from ..adjoint import default_segment, strain_fields
-            k = default_segment(self.nt, mode, 1, g)
-            # checkpoints, segment stores (strain, divergence), and the adjoint's own wavefields
-            return b + (-(-self.nt // k) * (ns + 2 * nv) + k * (strain_fields(mode) + nv) + 2 * ns + 3 * nv) * field
+            from ..adjoint import fixed_bytes
+            # checkpoints, segment stores, both batches' wavefields, traces, data and trace gradients
+            return fixed_bytes(self.nt, mode, 1, g, self.nrec)
+        b = (2 * ns + 3 * nv) * field + 4 * self.nrec * self.nt * nv * 3
         if snapshots:
             b += self.nsa * min(nv, 2) * field * (2 if (mode != FWI_SH and self.kernel_rho) else 1)
         return b

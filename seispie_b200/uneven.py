@@ -5,14 +5,13 @@ and nt.  Instances of one wave type share one launch per time step
 (fwi_multi_run); the whole time loop of every wave type can be captured into
 one CUDA graph and replayed as a single launch.
 
-    python -m seispie_b200.uneven [--instances 48] [--seed 0] [--check 150]
+    python -m seispie_b200.uneven [--instances 48] [--seed 0]
 
 runs the uneven-batch configuration (48 SH and P-SV instances, grids drawn
 from 128 to 768 cells a side with aspect 1:1 to 2:1, nt 1500-6000, 8-32
 shots, smooth-plus-checkerboard models seeded per instance) and prints one
-JSON line: throughput, HBM roofline of the step launches, and each
-instance's relative L2 trace error over its first --check steps against the
-FP64 oracle (computed on the host; skipped with --check 0).
+JSON line: throughput and HBM roofline of the step launches.  The traces'
+errors against the FP64 oracle are checked by tests/test_gpu_uneven.py.
 """
 from __future__ import annotations
 
@@ -20,7 +19,6 @@ import argparse
 import ctypes
 import json
 import os
-import sys
 import time
 from dataclasses import dataclass, field
 
@@ -93,7 +91,7 @@ class UnevenBatch:
             m = build_model(inst.mode, g, inst.dt, inst.params, inst.absorb, device)
             sid = point_ids(inst.src, np.float32(inst.h), np.float32(inst.h), inst.nz)
             rid = point_ids(inst.rec, np.float32(inst.h), np.float32(inst.h), inst.nz)
-            b = ShotBatch(m, len(sid), inst.nt, rid, tile=tile)
+            b = ShotBatch(m, len(sid), inst.nt, rid, tile=tile, displacement=True)
             stf, par = ricker_stf(inst.src, inst.nt, inst.dt, device)
             d = b.desc(inj=injection_lists(len(sid), sid, lambda s: s), stf=stf)
             d._stf = (stf, par)
@@ -151,34 +149,10 @@ class UnevenBatch:
         return [b.traces(c) if b.obs[c] is not None else None for c in range(3)]
 
 
-def oracle_error(inst: Instance, traces, nsteps: int, shot: int = 0) -> float:
-    """Relative L2 error of one shot's first nsteps trace samples against the
-    FP64 oracle run for nsteps steps (host)."""
-    from oracle.oracle import Oracle, point_ids as opids, source_time_functions
-    o = Oracle("f64")
-    lam, mu = o.vps2lm(inst.params["vp"], inst.params["vs"], inst.params["rho"])
-    p = dict(rho=inst.params["rho"], lam=lam, mu=mu, bound=o.set_bound(inst.nx, inst.nz, *inst.absorb))
-    h = np.float32(inst.h)
-    sid = opids(inst.src, h, h, inst.nz)
-    rid = opids(inst.rec, h, h, inst.nz)
-    stf = source_time_functions(inst.src, nsteps, inst.dt)
-    obs, _, _ = o.forward(inst.mode, inst.nx, inst.nz, float(h), float(h), inst.dt, nsteps, p, sid, stf, shot, rid)
-    num = den = 0.0
-    for c in range(3):
-        if traces[c] is None:
-            continue
-        got = traces[c][shot, :, :nsteps].double().cpu().numpy().reshape(-1)
-        ref = obs["xyz"[c]].reshape(len(rid), nsteps).reshape(-1)
-        num += float(np.sum((got - ref) ** 2))
-        den += float(np.sum(ref ** 2))
-    return (num / den) ** 0.5 if den > 0 else 0.0
-
-
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--instances", type=int, default=48)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--check", type=int, default=150, help="steps of the per-instance oracle check (0 = skip)")
     ap.add_argument("--tile", type=int, default=0)
     ap.add_argument("--reps", type=int, default=1)
     a = ap.parse_args(argv)
@@ -203,19 +177,12 @@ def main(argv=None):
                                                  "MEASURED_PEAKS.json")))["hbm_gbs"])
     except Exception:
         pass
-    errs = []
-    if a.check:
-        sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
-        for k, inst in enumerate(insts):
-            errs.append(oracle_error(inst, ub.traces(k), min(a.check, inst.nt)))
     line = {"metric": "Gcell-updates/s (uneven batch, one graph launch)", "value": cells / sec / 1e9,
             "unit": "Gcell-updates/s", "instances": len(insts), "cells": cells, "seconds": sec,
             "graph_launches_per_run": 1, "kernel_launches_per_run": ub.launch_count_per_run(),
             "roofline": {"bound": "hbm", "achieved": bytes_ / sec / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": bytes_ / sec / 1e9 / peak},
-            "max_rel_err_vs_fp64_oracle": max(errs) if errs else None, "oracle_check_steps": a.check,
-            "per_instance": [dict(mode=i.mode, nx=i.nx, nz=i.nz, nt=i.nt, shots=len(i.src),
-                                  err=(errs[k] if errs else None)) for k, i in enumerate(insts)]}
+            "per_instance": [dict(mode=i.mode, nx=i.nx, nz=i.nz, nt=i.nt, shots=len(i.src)) for i in insts]}
     print(json.dumps(line))
     return line
 

@@ -3,10 +3,11 @@
 Runs icui/seispie's own ``seispie.solver.fd2d`` plugin, unchanged, under
 Numba's CUDA simulator (NUMBA_ENABLE_CUDASIM=1), on grids small enough for the
 simulator (about 1e3 cell-updates/s), and saves inputs and outputs as .npz.
-The reference is read from REFERENCE (default /root/reference); it only has
-to exist when this script runs, never when the tests run.
+The reference checkout is named by --reference (or the SEISPIE_REFERENCE
+environment variable); it only has to exist when this script runs, never when
+the tests run.
 
-    python tests/golden/make_golden.py [--only NAME ...]
+    python tests/golden/make_golden.py --reference PATH [--only NAME ...]
 
 Each case drives the plugin exactly as sprun would (scripts/sprun:79-86):
 ``config`` is a dict of strings, ``path`` a dict of paths, ``mpi`` is None.
@@ -20,8 +21,7 @@ import tempfile
 import time
 
 os.environ["NUMBA_ENABLE_CUDASIM"] = "1"
-REFERENCE = os.environ.get("SEISPIE_REFERENCE", "/root/reference")
-sys.path.insert(0, REFERENCE)
+REFERENCE = None  # set from --reference / SEISPIE_REFERENCE before any case runs
 
 import numpy as np  # noqa: E402
 
@@ -334,8 +334,14 @@ CASES = dict(optimize=case_optimize, sh_fwd=case_sh_fwd, psv_fwd=case_psv_fwd, s
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=os.environ.get("SEISPIE_REFERENCE"),
+                    help="root of the seispie checkout to run (the directory holding the seispie package)")
     ap.add_argument("--only", nargs="*", default=None)
     args = ap.parse_args()
+    if not args.reference or not os.path.isdir(os.path.join(args.reference, "seispie")):
+        ap.error("--reference (or SEISPIE_REFERENCE) must name the seispie checkout")
+    REFERENCE = os.path.abspath(args.reference)
+    sys.path.insert(0, REFERENCE)
     for name, fn in CASES.items():
         if args.only is None or name in args.only:
             fn()

@@ -23,8 +23,28 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_library_is_built_for_sm100a():
-    out = subprocess.run(["cuobjdump", "--list-elf", _lib.lib_path()], capture_output=True, text=True).stdout
-    assert "sm_100a" in out
+    """Every translation unit was compiled for sm_100a only (the commands
+    build.py recorded), and the link used the same target."""
+    import json
+    import os
+    from seispie_b200 import build
+    _lib.load()
+    assert os.path.exists(build.INFO), "built without build.py's record"
+    info = json.load(open(build.INFO))
+    assert len(info["compile"]) == len(build.SOURCES)
+    for cmd in info["compile"] + [info["link"]]:
+        assert "arch=compute_100a,code=sm_100a" in cmd
+        assert cmd.count("-gencode") == 1
+
+
+@pytest.mark.gpu
+def test_loaded_device_code_is_sm100():
+    """The device code the runtime loaded reports binary version 100."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    torch.cuda.init()
+    assert _lib.load().fwi_binary_version() == 100
 
 
 def _err():

@@ -375,14 +375,17 @@ def test_two_level_checkpointing_is_bit_identical(mode):
                dict(segment=37, tail_memory=61.5 * per_step)):
         ea = ExactAdjoint(m, nt, setup.src_id, setup.isrc_of_shot, setup.nshots, setup.stf, setup.rec_id, **kw)
         tr = ea.forward()
-        out.append((tr, ea.backward(g)))
+        out.append((tr, ea.backward(g), ea.illum.clone()))
         if "tail_memory" in kw:
             assert ea.tail == 61 and ea.t0 == nt - 61
-    (tr1, k1) = out[0]
+    (tr1, k1, il1) = out[0]
     assert len(k1) == (6 if mode == "spin" else 3)
-    for tr2, k2 in out[1:]:
+    for tr2, k2, _ in out[1:]:
         for c in (0, 2):
             assert torch.equal(tr1[c], tr2[c])
         for a, b in zip(k1, k2):
             assert torch.equal(a, b)
     assert float(k1[1].abs().max()) > 0
+    # the illumination is sampled at the multiples of the segment whether or not a stored tail
+    # takes the last steps, so it does not depend on the memory the tail got
+    assert torch.equal(il1, out[2][2]) and float(il1.max()) > 0

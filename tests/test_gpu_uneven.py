@@ -60,10 +60,8 @@ def test_uneven_batch_matches_single_runs_bitwise():
 
 
 def test_uneven_batch_vs_fp64_oracle():
-    import os
-    import sys
-    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
-    from seispie_b200.uneven import UnevenBatch, oracle_error
+    from seispie_b200.uneven import UnevenBatch
+    from tests.gpu_helpers import oracle_trace_error as oracle_error
     insts = _small_instances()
     ub = UnevenBatch(insts)
     ub.prepare()

@@ -122,11 +122,15 @@ def test_exact_adjoint_fixed_bytes():
     from seispie_b200.engine import Grid
     g = Grid(1024, 510, 10.0, 10.0)  # pitch 512
     field = 4 * 64 * 1024 * 512
+    # displacement-free P-SV: a checkpoint is 3 stress + 2 velocity fields, a step stores
+    # 3 strain terms and 2 divergences, so K = sqrt(nt)
     k = default_segment(6000, FWI_PSV, 64, g)
-    assert k == 92
-    want = (66 * 7 + 92 * 5 + 2 * 7) * field + 3 * 4 * 64 * 256 * 6000
+    assert k == 77
+    # 78 checkpoints, 77 steps of stores, forward and adjoint batches of 2 x (3 + 2) fields,
+    # and 2 components x (traces, data, trace gradients)
+    want = (78 * 5 + 77 * 5 + 2 * 10) * field + 3 * 4 * 64 * 256 * 6000 * 2
     assert fixed_bytes(6000, FWI_PSV, 64, g, 256) == want
     # an explicit segment; the spin state is 6 stress + 2 x 3 velocity/displacement fields,
-    # and a step stores 6 strain terms and 3 divergences
+    # a step stores 6 strain terms and 3 divergences, a batch holds 2 x (6 + 3) + 3 fields
     assert fixed_bytes(100, FWI_SPIN, 2, Grid(8, 8, 1.0, 1.0), 0, segment=10) == \
-        (10 * 12 + 10 * 9 + 2 * 12) * 4 * 2 * 8 * 8
+        (10 * 12 + 10 * 9 + 2 * 21) * 4 * 2 * 8 * 8
