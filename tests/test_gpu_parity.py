@@ -114,7 +114,15 @@ def test_displacement_free_bit_identical(mode, nx, nz, nshots):
     multiple of 4, nz near the 1024-column limit, a 5-row grid, more shots
     than sources (isrc -1: all of them), the time loop in several calls."""
     isrcs = [(-1 if s % 3 == 2 else s % 3) for s in range(nshots)]
-    _march_vs_tiled(mode, nx, nz, isrcs, 70, seed=nx + nz, chunks=[1, 23, 46])
+    h = 10.0
+    # sources and receivers spread over the grid, receivers a few cells from the sources
+    src = np.array([[(nx // 2) * h, (nz // 3) * h, 0, 12.0, 0.08, 30.0, 1e10],
+                    [(nx // 3) * h, (nz // 2) * h, 0, 10.0, 0.1, -60.0, 1e10],
+                    [(nx - 1) * h, 2 * h, 0, 14.0, 0.07, 0.0, 1e10]])
+    rec = np.array([[0, 0], [(nx - 1) * h, (nz - 1) * h], [0, (nz - 1) * h], [(nx - 1) * h, 5 * h]] +
+                   [[min(nx - 1, nx // 2 + d) * h, min(nz - 1, nz // 3 + 3 * d) * h] for d in range(4)] +
+                   [[(nx // 3) * h, min(nz - 1, nz // 2 + d) * h] for d in (-2, 1, 4)])
+    _march_vs_tiled(mode, nx, nz, isrcs, 70, seed=nx + nz, chunks=[1, 23, 46], src=src, rec=rec)
 
 
 def test_displacement_free_bit_identical_full_size():
