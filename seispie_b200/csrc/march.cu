@@ -6,20 +6,21 @@
 // layout that keeps the instruction count per cell low enough for the step to
 // be bound by HBM rather than by issue:
 //
-//   * A CTA spans the whole z extent of the grid (thread j = column j, up to
-//     1024 columns) and marches down a contiguous range of x rows of one
-//     shot.  The 4th-order x derivatives come from register windows of four
-//     rows, the z derivatives from the neighbouring columns of the current
-//     row in shared memory, so every value is loaded from shared memory once
-//     per row and there is no 2-D index arithmetic per cell.
-//   * Rows of the state (stress, velocity) stream into a ring of row slots in
-//     shared memory with untiled bulk copies (cp.async.bulk, one per field
+//   * A CTA spans the whole z extent of the grid -- thread t owns the four
+//     columns 4t .. 4t+3 (up to 1024 columns) -- and marches down a
+//     contiguous range of x rows of one shot.  Every shared-memory access
+//     and every store is a 16-byte vector for four cells; the z neighbours
+//     come from one 8- and one 4-byte load beside it.  The 4th-order x
+//     derivatives of the stress come from register windows of four rows.
+//   * Rows of the state (stress, velocity) stream into a ring of N row slots
+//     in shared memory with untiled bulk copies (cp.async.bulk, one per field
 //     and row, completion on an mbarrier per slot, bounded waits), issued by
-//     one thread several rows ahead of the march.  The model, shared by the
-//     shots and resident in L2, is read with ordinary loads one row ahead.
-//   * The new velocity of row r goes to a four-row ring in shared memory;
-//     the stress of row r-2 is updated in the same iteration from the
-//     velocity window (D+x) and that ring (D+z).  One block barrier per row.
+//     one thread N-1 rows ahead of the march.  The model, shared by the shots
+//     and resident in L2, is read with 16-byte loads one row ahead.
+//   * The new velocity of row r goes to an eight-row ring in shared memory;
+//     the stress of row r-2 is updated in the same iteration from that ring
+//     (rows r-3 .. r for D+x, row r-2's neighbours for D+z).  One block
+//     barrier per row.
 //   * The rows of all shots form one sequence, split evenly over a grid of
 //     resident CTAs (one pass, no tail wave); a CTA whose range starts in
 //     the middle of a shot recomputes the velocity of the row above its range
@@ -58,12 +59,13 @@ int march_device_status(int clear, int *status) {
     return 0;
 }
 
-constexpr int kPts = 256;       // points (injection entries, receivers) staged per window
-constexpr int kMaxCols = 1024;  // z extent a CTA can span (one thread per column)
+constexpr int kPts = 256;        // points (injection entries, receivers) staged per window
+constexpr int kMaxPitch = 1024;  // row length (floats) a CTA can span: 256 threads of 4 columns
+constexpr int kVRing = 8;        // rows of the new-velocity ring
 
 struct MarchArgs {
     int nx, nz, pitch, nt, it, nrec;
-    int rl, nslots;         // shared-memory row length (floats) and ring depth
+    int rl;                 // shared-memory row length (floats)
     long long rows_total;   // nshots * nx
     float cx1, cx2, cz1, cz2, dt;
     const float *sig_in[3];
@@ -81,8 +83,8 @@ struct MarchArgs {
 };
 
 // Shared-memory layout, in floats: ring [nslots][NF][rl], velocity ring
-// [4][NV][rl], injection window (cells, NINJ value rows), receiver window
-// (cells, ids), two cursors, then the mbarriers (8-byte aligned).
+// [kVRing][NV][rl], injection window (cells, NINJ value rows), receiver
+// window (cells, ids), two cursors, then the mbarriers (8-byte aligned).
 struct MarchLayout {
     int vring, icell, ival, rcell, rid, cur, bar;
     size_t bytes;
@@ -91,7 +93,7 @@ struct MarchLayout {
 __host__ __device__ inline MarchLayout march_layout(int nf, int nv, int ninj, int rl, int nslots) {
     MarchLayout L;
     L.vring = nslots * nf * rl;
-    L.icell = L.vring + 4 * nv * rl;
+    L.icell = L.vring + kVRing * nv * rl;
     L.ival = L.icell + kPts;
     L.rcell = L.ival + ninj * kPts;
     L.rid = L.rcell + kPts;
@@ -123,12 +125,33 @@ struct Cursor {
 };
 constexpr int kNone = 0x7fffffff;  // "no further point"
 
-template <int MODE>
-__global__ void __launch_bounds__(kMaxCols) march_kernel(const __grid_constant__ MarchArgs a) {
+__device__ __forceinline__ void ld4(float (&d)[4], const float *p) {
+    const float4 v = *reinterpret_cast<const float4 *>(p);
+    d[0] = v.x;
+    d[1] = v.y;
+    d[2] = v.z;
+    d[3] = v.w;
+}
+__device__ __forceinline__ void st4(float *p, const float (&d)[4]) {
+    *reinterpret_cast<float4 *>(p) = make_float4(d[0], d[1], d[2], d[3]);
+}
+__device__ __forceinline__ void ldg4(float (&d)[4], const float *p) {
+    const float4 v = __ldg(reinterpret_cast<const float4 *>(p));
+    d[0] = v.x;
+    d[1] = v.y;
+    d[2] = v.z;
+    d[3] = v.w;
+}
+
+template <int MODE, int N>
+__global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_constant__ MarchArgs a) {
     using F = Fields<MODE>;
     constexpr int NS = F::NS, NV = F::NV, NF = NS + NV, NINJ = F::NINJ;
+    // stress fields with an x register window (D-x) and the one without
+    constexpr int FX0 = 0, FX1 = MODE == FWI_SH ? 0 : 2, FZ = 1;
+    constexpr int NW = MODE == FWI_SH ? 1 : 2;
     extern __shared__ __align__(128) float smem[];
-    const int RL = a.rl, N = a.nslots;
+    const int RL = a.rl;
     const MarchLayout L = march_layout(NF, NV, NINJ, RL, N);
     int *const i_cell = reinterpret_cast<int *>(smem + L.icell);
     float *const i_val = smem + L.ival;
@@ -137,14 +160,14 @@ __global__ void __launch_bounds__(kMaxCols) march_kernel(const __grid_constant__
     Cursor *const cur_s = reinterpret_cast<Cursor *>(smem + L.cur);  // [0] injection, [1] receivers
     uint64_t *const full = reinterpret_cast<uint64_t *>(smem + L.bar);
 
-    const int tid = threadIdx.x, j = tid;
+    const int tid = threadIdx.x, j0 = 4 * tid;
     const int nx = a.nx, nz = a.nz, pitch = a.pitch, nt = a.nt, it = a.it;
-    const bool jin = j < nz;
+    const bool tin = j0 < pitch;  // this thread's four columns lie in the rows
     const float cx1 = a.cx1, cx2 = a.cx2, cz1 = a.cz1, cz2 = a.cz2, dt = a.dt;
     const uint32_t row_bytes = 4u * (uint32_t)pitch;
     // row buffers start 4 floats into their slot so that columns -4 .. rl-5 are addressable
     auto ring_row = [&](int slot, int f) -> float * { return smem + (slot * NF + f) * RL + 4; };
-    auto vel_row = [&](int k, int c) -> float * { return smem + L.vring + (k * NV + c) * RL + 4; };
+    auto vel_row = [&](int row, int c) -> float * { return smem + L.vring + ((row & (kVRing - 1)) * NV + c) * RL + 4; };
 
     if (tid == 0) {
         for (int i = 0; i < N; i++) mbar_init(&full[i], 1);
@@ -213,6 +236,15 @@ __global__ void __launch_bounds__(kMaxCols) march_kernel(const __grid_constant__
         __syncthreads();
         return nxt;
     };
+    // model row `row` at this thread's columns (zero outside the grid)
+    auto ld_model = [&](float (&d)[4], const float *p, int row) {
+        if (tin && row >= 0 && row < nx) {
+            ldg4(d, p + (long long)row * pitch + j0);
+        } else {
+#pragma unroll
+            for (int e = 0; e < 4; e++) d[e] = 0.f;
+        }
+    };
 
     while (Lrow < Lend) {
         const int shot = Lrow / nx, a0 = Lrow - shot * nx;
@@ -248,32 +280,33 @@ __global__ void __launch_bounds__(kMaxCols) march_kernel(const __grid_constant__
         }
 
         bool ok = true;
-        // register windows: stress rows r-2 .. r+1 (SH: sxy, szy; P-SV: sxx, szz, sxz),
-        // new velocity rows r-3 .. r
-        float ws[NS][4], wv[NV][4];
+        // register windows of four cells: the D-x stress fields at rows
+        // r-2 .. r+1 (SH: sxy; P-SV: sxx, sxz), the other stress field at rows
+        // r-2 .. r (SH: szy; P-SV: szz)
+        float wx[NW][4][4], wz[3][4];
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             const int q = va - 2 + k;
             if (q >= qa) {
                 ok = wait_seq(sb + q) && ok;
                 const int sl = (sb + q) % N;
-#pragma unroll
-                for (int f = 0; f < NS; f++) ws[f][k] = ring_row(sl, f)[j];
+                ld4(wx[0][k], ring_row(sl, FX0) + j0);
+                if (NW > 1) ld4(wx[NW - 1][k], ring_row(sl, FX1) + j0);
+                if (k < 2) ld4(wz[k + 1], ring_row(sl, FZ) + j0);  // rows va-2, va-1 -> wz[1], wz[2]
             } else {
 #pragma unroll
-                for (int f = 0; f < NS; f++) ws[f][k] = 0.f;
+                for (int e = 0; e < 4; e++) {
+                    wx[0][k][e] = wx[NW - 1][k][e] = 0.f;
+                    if (k < 2) wz[k + 1][e] = 0.f;
+                }
             }
         }
-#pragma unroll
-        for (int c = 0; c < NV; c++)
-#pragma unroll
-            for (int k = 0; k < 4; k++) wv[c][k] = 0.f;
         // model of the first row: dt/rho and sponge (row va), stiffness (row va-2)
-        auto ld_model = [&](const float *p, int row) -> float {
-            return (jin && row >= 0 && row < nx) ? __ldg(p + (long long)row * pitch + j) : 0.f;
-        };
-        float buo = ld_model(a.buo, va), bnd = ld_model(a.bound, va);
-        float ip0 = ld_model(a.ip[0], va - 2), ip1 = MODE == FWI_PSV ? ld_model(a.ip[1], va - 2) : 0.f;
+        float buo[4], bnd[4], ip0[4], ip1[4];
+        ld_model(buo, a.buo, va);
+        ld_model(bnd, a.bound, va);
+        ld_model(ip0, a.ip[0], va - 2);
+        if (MODE == FWI_PSV) ld_model(ip1, a.ip[1], va - 2);
         if (__syncthreads_or(!ok)) goto bail;
         // rows above va are consumed: their slots take the next rows
         for (int q = qa; q < va; q++)
@@ -284,68 +317,110 @@ __global__ void __launch_bounds__(kMaxCols) march_kernel(const __grid_constant__
 
         for (int r = va; r < b0 + 2; r++) {
             // next iteration's model values (one row ahead)
-            const float buo_n = ld_model(a.buo, r + 1), bnd_n = ld_model(a.bound, r + 1);
-            const float ip0_n = ld_model(a.ip[0], r - 1);
-            const float ip1_n = MODE == FWI_PSV ? ld_model(a.ip[1], r - 1) : 0.f;
-            float vn[NV];
+            float buo_n[4], bnd_n[4], ip0_n[4], ip1_n[4];
+            ld_model(buo_n, a.buo, r + 1);
+            ld_model(bnd_n, a.bound, r + 1);
+            ld_model(ip0_n, a.ip[0], r - 1);
+            if (MODE == FWI_PSV) ld_model(ip1_n, a.ip[1], r - 1);
+            // the z window shifts: wz[0..2] <- rows r-2, r-1, r
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                wz[0][e] = wz[1][e];
+                wz[1][e] = wz[2][e];
+            }
+            float vn[NV][4];
+            const long long grow = soff + (long long)r * pitch + j0;
             if (r < vb) {
                 // ---- velocity of row r
                 if (r + 1 < qb) {
                     ok = wait_seq(sb + r + 1) && ok;
                     const int sl = (sb + r + 1) % N;
-#pragma unroll
-                    for (int f = 0; f < NS; f++) ws[f][3] = ring_row(sl, f)[j];
+                    ld4(wx[0][3], ring_row(sl, FX0) + j0);
+                    if (NW > 1) ld4(wx[NW - 1][3], ring_row(sl, FX1) + j0);
                 } else {
 #pragma unroll
-                    for (int f = 0; f < NS; f++) ws[f][3] = 0.f;
+                    for (int e = 0; e < 4; e++) wx[0][3][e] = wx[NW - 1][3][e] = 0.f;
                 }
                 const int sr = (sb + r) % N;
-                const bool okx = r >= 2 && r < nx - 2, okz = j >= 2 && j < nz - 2;
-                auto dxm = [&](int f) -> float {
-                    return okx ? cx1 * (ws[f][2] - ws[f][1]) - cx2 * (ws[f][3] - ws[f][0]) : 0.f;
+                ld4(wz[2], ring_row(sr, FZ) + j0);
+                const bool okx = r >= 2 && r < nx - 2;
+                // D-x of window field w, element e
+                auto dxm = [&](int w, int e) -> float {
+                    return okx ? cx1 * (wx[w][2][e] - wx[w][1][e]) - cx2 * (wx[w][3][e] - wx[w][0][e]) : 0.f;
                 };
-                auto dzm = [&](int f) -> float {
-                    const float *s = ring_row(sr, f) + j;
-                    return okz ? cz1 * (ws[f][2] - s[-1]) - cz2 * (s[1] - s[-2]) : 0.f;
+                // D-z of stress field f at row r, element e, from columns j0-2 .. j0+4:
+                // x[i] = column j0-2+i, with the centre taken from `cen`
+                auto dzm_row = [&](int f, const float (&cen)[4], float (&out)[4]) {
+                    const float *s = ring_row(sr, f) + j0;
+                    const float2 l2 = *reinterpret_cast<const float2 *>(s - 2);
+                    const float rr = s[4];
+                    const float x[7] = {l2.x, l2.y, cen[0], cen[1], cen[2], cen[3], rr};
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        const int c = j0 + e;
+                        const bool okz = c >= 2 && c < nz - 2;
+                        out[e] = okz ? cz1 * (x[e + 2] - x[e + 1]) - cz2 * (x[e + 3] - x[e]) : 0.f;
+                    }
                 };
-                float ds[NV];
+                float ds[NV][4];
                 if constexpr (MODE == FWI_SH) {
-                    ds[0] = dxm(0) + dzm(1);
+                    float zm[4];
+                    dzm_row(1, wz[2], zm);
+#pragma unroll
+                    for (int e = 0; e < 4; e++) ds[0][e] = dxm(0, e) + zm[e];
                 } else {
-                    ds[0] = dxm(0) + dzm(2);
-                    ds[1] = dxm(2) + dzm(1);
+                    float zxz[4], zzz[4];
+                    dzm_row(2, wx[1][2], zxz);
+                    dzm_row(1, wz[2], zzz);
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        ds[0][e] = dxm(0, e) + zxz[e];
+                        ds[1][e] = dxm(1, e) + zzz[e];
+                    }
                 }
                 // sources of row r, summed per cell in entry order (stf_dsy / stf_dsxz, solver.py:78-93)
                 if (inj_next < (r + 1) * nz) {
                     const int lo = r * nz, hi = lo + nz;
-                    float acc[NINJ];
+                    float acc[NINJ][4];
 #pragma unroll
-                    for (int q = 0; q < NINJ; q++) acc[q] = 0.f;
+                    for (int q = 0; q < NINJ; q++)
+#pragma unroll
+                        for (int e = 0; e < 4; e++) acc[q][e] = 0.f;
                     Cursor c = cur_s[0];
                     while (c.p < c.end) {
                         if (c.p - c.w0 >= c.wn) load_inj(c);
                         const int k = c.p - c.w0, cell = i_cell[k];
                         if (cell >= hi) break;
-                        if (cell - lo == j) {
+                        const int off = cell - lo - j0;
 #pragma unroll
-                            for (int q = 0; q < NINJ; q++) acc[q] += i_val[q * kPts + k];
-                        }
+                        for (int e = 0; e < 4; e++)
+                            if (off == e) {
+#pragma unroll
+                                for (int q = 0; q < NINJ; q++) acc[q][e] += i_val[q * kPts + k];
+                            }
                         c.p++;
                     }
                     inj_next = park(c, 0, true);
 #pragma unroll
-                    for (int q = 0; q < NV; q++) ds[q] += acc[q];
+                    for (int q = 0; q < NV; q++)
+#pragma unroll
+                        for (int e = 0; e < 4; e++) ds[q][e] += acc[q][e];
                 }
-                const long long g = soff + (long long)r * pitch + j;
-                const bool own = r >= a0 && r < b0 && jin;
+                const bool own = r >= a0 && r < b0 && tin;
 #pragma unroll
                 for (int c = 0; c < NV; c++) {
-                    const float vold = ring_row(sr, NS + c)[j];
-                    vn[c] = bnd * (vold + ds[c] * buo);
-                    vel_row(r & 3, c)[j] = vn[c];
+                    float vold[4];
+                    ld4(vold, ring_row(sr, NS + c) + j0);
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        const float v = bnd[e] * (vold[e] + ds[c][e] * buo[e]);
+                        vn[c][e] = j0 + e < nz ? v : 0.f;  // padding columns stay zero
+                        if (j0 + e >= nz) ds[c][e] = 0.f;
+                    }
+                    st4(vel_row(r, c) + j0, vn[c]);
                     if (own) {
-                        a.vel_out[c][g] = vn[c];
-                        if (a.seg_ds[c]) a.seg_ds[c][g] = ds[c];
+                        st4(a.vel_out[c] + grow, vn[c]);
+                        if (a.seg_ds[c]) st4(a.seg_ds[c] + grow, ds[c]);
                     }
                 }
                 // receivers of row r record the new velocity (save_obs, solver.py:151-156)
@@ -356,11 +431,16 @@ __global__ void __launch_bounds__(kMaxCols) march_kernel(const __grid_constant__
                         if (c.p - c.w0 >= c.wn) load_rec(c);
                         const int k = c.p - c.w0, cell = r_cell[k];
                         if (cell >= hi) break;
-                        if (cell - lo == j) {
+                        const int off = cell - lo - j0;
+                        if (off >= 0 && off < 4) {
                             const long long o = ((long long)shot * a.nrec + r_id[k]) * nt + it;
 #pragma unroll
-                            for (int q = 0; q < NV; q++)
-                                if (a.obs[q]) a.obs[q][o] = vn[q];
+                            for (int e = 0; e < 4; e++)
+                                if (off == e) {
+#pragma unroll
+                                    for (int q = 0; q < NV; q++)
+                                        if (a.obs[q]) a.obs[q][o] = vn[q][e];
+                                }
                         }
                         c.p++;
                     }
@@ -369,19 +449,13 @@ __global__ void __launch_bounds__(kMaxCols) march_kernel(const __grid_constant__
             } else {
 #pragma unroll
                 for (int c = 0; c < NV; c++) {
-                    vn[c] = 0.f;
-                    vel_row(r & 3, c)[j] = 0.f;
+#pragma unroll
+                    for (int e = 0; e < 4; e++) vn[c][e] = 0.f;
+                    st4(vel_row(r, c) + j0, vn[c]);
                 }
             }
-#pragma unroll
-            for (int c = 0; c < NV; c++) {
-                wv[c][0] = wv[c][1];
-                wv[c][1] = wv[c][2];
-                wv[c][2] = wv[c][3];
-                wv[c][3] = vn[c];
-            }
             if (__syncthreads_or(!ok)) goto bail;
-            // row r is consumed: its slot takes row r + nslots
+            // row r is consumed: its slot takes row r + N
             if (nexti < qb) {
                 if (tid == 0) issue(soff, nexti, sb + nexti);
                 nexti++;
@@ -389,48 +463,84 @@ __global__ void __launch_bounds__(kMaxCols) march_kernel(const __grid_constant__
 
             // ---- stress of row s = r - 2 (add_sy / add_sxz, solver.py:128-149)
             const int s = r - 2;
-            if (s >= a0 && s < b0 && jin) {
-                const bool okx = s >= 1 && s < nx - 2, okz = j >= 1 && j < nz - 2;
-                auto dxp = [&](int c) -> float {
-                    return okx ? cx1 * (wv[c][2] - wv[c][1]) - cx2 * (wv[c][3] - wv[c][0]) : 0.f;
-                };
-                auto dzp = [&](int c) -> float {
-                    const float *v = vel_row(s & 3, c) + j;
-                    return okz ? cz1 * (v[1] - wv[c][1]) - cz2 * (v[2] - v[-1]) : 0.f;
-                };
-                const long long g = soff + (long long)s * pitch + j;
+            if (s >= a0 && s < b0 && tin) {
+                const bool okx = s >= 1 && s < nx - 2;
+                const long long gs = soff + (long long)s * pitch + j0;
+                float ex[NV][4], ez[NV][4];
+#pragma unroll
+                for (int c = 0; c < NV; c++) {
+                    // rows s-1 .. s+2 of the new velocity, and row s's z neighbours:
+                    // y[i] = column j0-1+i of row s
+                    float v0[4], v1[4], v2[4], v3[4];
+                    ld4(v0, vel_row(s - 1, c) + j0);
+                    ld4(v1, vel_row(s, c) + j0);
+                    ld4(v2, vel_row(s + 1, c) + j0);
+                    ld4(v3, vel_row(s + 2, c) + j0);
+                    const float *vs = vel_row(s, c) + j0;
+                    const float l1 = vs[-1];
+                    const float2 r2 = *reinterpret_cast<const float2 *>(vs + 4);
+                    const float y[7] = {l1, v1[0], v1[1], v1[2], v1[3], r2.x, r2.y};
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        const int cc = j0 + e;
+                        const bool okz = cc >= 1 && cc < nz - 2;
+                        ex[c][e] = okx ? cx1 * (v2[e] - v1[e]) - cx2 * (v3[e] - v0[e]) : 0.f;
+                        ez[c][e] = okz ? cz1 * (y[e + 2] - y[e + 1]) - cz2 * (y[e + 3] - y[e]) : 0.f;
+                    }
+                }
                 if constexpr (MODE == FWI_SH) {
-                    const float dm = dt * ip0, exy = dxp(0), ezy = dzp(0);
-                    a.sig_out[0][g] = ws[0][0] + dm * exy;
-                    a.sig_out[1][g] = ws[1][0] + dm * ezy;
+                    float o0[4], o1[4];
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        const float dm = dt * ip0[e], exy = ex[0][e], ezy = ez[0][e];
+                        const bool in = j0 + e < nz;  // padding columns stay zero
+                        o0[e] = in ? wx[0][0][e] + dm * exy : 0.f;
+                        o1[e] = in ? wz[0][e] + dm * ezy : 0.f;
+                    }
+                    st4(a.sig_out[0] + gs, o0);
+                    st4(a.sig_out[1] + gs, o1);
                     if (a.seg_e[0]) {
-                        a.seg_e[0][g] = exy;
-                        a.seg_e[1][g] = ezy;
+                        st4(a.seg_e[0] + gs, ex[0]);
+                        st4(a.seg_e[1] + gs, ez[0]);
                     }
                 } else {
-                    const float lam = ip0, mu = ip1;
-                    const float vxx = dxp(0), vxz = dzp(0), vzx = dxp(1), vzz = dzp(1);
-                    const float l2m = lam + 2.f * mu, shear = vxz + vzx;
-                    a.sig_out[0][g] = ws[0][0] + dt * (l2m * vxx + lam * vzz);
-                    a.sig_out[1][g] = ws[1][0] + dt * (l2m * vzz + lam * vxx);
-                    a.sig_out[2][g] = ws[2][0] + dt * (mu * shear);
+                    float o0[4], o1[4], o2[4], sh[4];
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        const float lam = ip0[e], mu = ip1[e];
+                        const float vxx = ex[0][e], vxz = ez[0][e], vzx = ex[1][e], vzz = ez[1][e];
+                        const float l2m = lam + 2.f * mu, shear = vxz + vzx;
+                        const bool in = j0 + e < nz;  // padding columns stay zero
+                        o0[e] = in ? wx[0][0][e] + dt * (l2m * vxx + lam * vzz) : 0.f;
+                        o1[e] = in ? wz[0][e] + dt * (l2m * vzz + lam * vxx) : 0.f;
+                        o2[e] = in ? wx[1][0][e] + dt * (mu * shear) : 0.f;
+                        sh[e] = in ? shear : 0.f;
+                    }
+                    st4(a.sig_out[0] + gs, o0);
+                    st4(a.sig_out[1] + gs, o1);
+                    st4(a.sig_out[2] + gs, o2);
                     if (a.seg_e[0]) {
-                        a.seg_e[0][g] = vxx;
-                        a.seg_e[1][g] = vzz;
-                        a.seg_e[2][g] = shear;
+                        st4(a.seg_e[0] + gs, ex[0]);
+                        st4(a.seg_e[1] + gs, ez[1]);
+                        st4(a.seg_e[2] + gs, sh);
                     }
                 }
             }
 #pragma unroll
-            for (int f = 0; f < NS; f++) {
-                ws[f][0] = ws[f][1];
-                ws[f][1] = ws[f][2];
-                ws[f][2] = ws[f][3];
+            for (int w = 0; w < NW; w++)
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    wx[w][0][e] = wx[w][1][e];
+                    wx[w][1][e] = wx[w][2][e];
+                    wx[w][2][e] = wx[w][3][e];
+                }
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                buo[e] = buo_n[e];
+                bnd[e] = bnd_n[e];
+                ip0[e] = ip0_n[e];
+                if (MODE == FWI_PSV) ip1[e] = ip1_n[e];
             }
-            buo = buo_n;
-            bnd = bnd_n;
-            ip0 = ip0_n;
-            ip1 = ip1_n;
         }
         continue;
     bail:
@@ -460,35 +570,34 @@ __global__ void displacement_traces_kernel(float *obs, long long ntr, int nt, in
 
 static int comp_slot_of(int mode, int q) { return mode == FWI_SH ? 1 : (q == 0 ? 0 : 2); }
 
-// Ring depth and bytes for a grid: as deep as 8 rows while two CTAs fit an
-// SM, else one CTA per SM; fewer than three slots is an error.
-static bool march_plan(int mode, int rl, int *nslots, size_t *bytes) {
+// Ring depth for a row length: 8 slots while two CTAs fit an SM, else 4
+// while two fit, else 8 with one CTA per SM.
+static int march_slots(int mode, int rl, size_t *bytes) {
     const int nf = mode == FWI_SH ? 3 : 5, nv = mode == FWI_SH ? 1 : 2, ninj = mode == FWI_SH ? 1 : 2;
-    const size_t budgets[2] = {(size_t)110 * 1024, (size_t)224 * 1024};
-    for (size_t budget : budgets) {
-        for (int n = 8; n >= 3; n--) {
-            const MarchLayout L = march_layout(nf, nv, ninj, rl, n);
-            if (L.bytes <= budget) {
-                *nslots = n;
-                *bytes = L.bytes;
-                return true;
-            }
-        }
+    const size_t two = (size_t)110 * 1024, one = (size_t)224 * 1024;
+    const size_t b8 = march_layout(nf, nv, ninj, rl, 8).bytes, b4 = march_layout(nf, nv, ninj, rl, 4).bytes;
+    if (b8 <= two || (b4 > two && b8 <= one)) {
+        *bytes = b8;
+        return 8;
     }
-    return false;
+    if (b4 <= one) {
+        *bytes = b4;
+        return 4;
+    }
+    return 0;
 }
 
 bool march_supported(const fwi_batch *b) {
-    return (b->mode == FWI_SH || b->mode == FWI_PSV) && b->nz <= kMaxCols;
+    return (b->mode == FWI_SH || b->mode == FWI_PSV) && b->pitch <= kMaxPitch;
 }
 
-template <int MODE>
+template <int MODE, int N>
 static int launch_march_mode(const MarchArgs &a, int nthr, size_t bytes, cudaStream_t st) {
     static size_t attr_bytes = 0;
     static int sms = 0, occ = 0, occ_thr = 0;
     static size_t occ_bytes = 0;
     if (bytes > attr_bytes) {
-        cudaError_t e = cudaFuncSetAttribute(march_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(march_kernel<MODE, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)bytes);
         if (e != cudaSuccess) return set_error(FWI_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
         attr_bytes = bytes;
@@ -500,7 +609,7 @@ static int launch_march_mode(const MarchArgs &a, int nthr, size_t bytes, cudaStr
             sms = 148;
     }
     if (occ_thr != nthr || occ_bytes != bytes) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, march_kernel<MODE>, nthr, bytes) != cudaSuccess ||
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, march_kernel<MODE, N>, nthr, bytes) != cudaSuccess ||
             occ < 1)
             return set_error(FWI_ECUDA, "march_kernel: %d threads with %zu bytes of shared memory do not fit an SM",
                              nthr, bytes);
@@ -508,7 +617,7 @@ static int launch_march_mode(const MarchArgs &a, int nthr, size_t bytes, cudaStr
         occ_bytes = bytes;
     }
     const long long grid = a.rows_total < (long long)sms * occ ? a.rows_total : (long long)sms * occ;
-    march_kernel<MODE><<<(unsigned)grid, nthr, bytes, st>>>(a);
+    march_kernel<MODE, N><<<(unsigned)grid, nthr, bytes, st>>>(a);
     return check_launch("march_kernel");
 }
 
@@ -558,15 +667,15 @@ int launch_march(const fwi_batch *b, int it, cudaStream_t st) {
     a.stf[1] = mode == FWI_SH ? nullptr : b->stf[2];
     a.rec_cell = b->rec_cell;
     a.rec_order = b->rec_order;
-    const int nthr = ((b->nz + 31) / 32) * 32 < 64 ? 64 : ((b->nz + 31) / 32) * 32;
-    int rl = (b->pitch > nthr ? b->pitch : nthr) + 8;
-    rl = (rl + 3) / 4 * 4;
-    a.rl = rl;
+    // four columns per thread, whole warps
+    const int nthr = ((b->pitch / 4 + 31) / 32) * 32;
+    a.rl = 4 * nthr + 8;
     size_t bytes = 0;
-    if (!march_plan(mode, rl, &a.nslots, &bytes))
-        return set_error(FWI_ERANGE, "row-marching step: rows of %d columns do not fit shared memory", b->pitch);
-    return mode == FWI_SH ? launch_march_mode<FWI_SH>(a, nthr, bytes, st)
-                          : launch_march_mode<FWI_PSV>(a, nthr, bytes, st);
+    const int n = march_slots(mode, a.rl, &bytes);
+    if (!n) return set_error(FWI_ERANGE, "row-marching step: rows of %d columns do not fit shared memory", b->pitch);
+    if (mode == FWI_SH)
+        return n == 8 ? launch_march_mode<FWI_SH, 8>(a, nthr, bytes, st) : launch_march_mode<FWI_SH, 4>(a, nthr, bytes, st);
+    return n == 8 ? launch_march_mode<FWI_PSV, 8>(a, nthr, bytes, st) : launch_march_mode<FWI_PSV, 4>(a, nthr, bytes, st);
 }
 
 // Binary version (major*10 + minor) of the device code the library loaded.
