@@ -286,22 +286,26 @@ class b200:
                     syn = tr[c].reshape(-1).contiguous()
                     misfit += float(engine.misfit_tracegrad(data, syn, grads[c], n, nrec, nt, self.dt).sum().item())
                     grads[c] = grads[c].view(n, nrec, nt)
-                ks = ea.backward(grads)
-                k_lam, k_mu, k_buo = ks[:3]
-                self.k_lam_f64 += self.dt * k_lam
-                self.k_mu_f64 += self.dt * k_mu
-                # buo = dt/rho: dchi/drho = -dchi/dbuo * dt / rho^2
-                rho = self.model.rho.double()
-                self.k_rho_f64 -= self.dt * k_buo * self.dt / torch.where(rho > 0, rho * rho, torch.ones_like(rho))
-                if mode == FWI_SPIN:
-                    # spin: nu, mu_c and nu_c (both through mnc = mu_c + nu_c), j through dt/j
-                    k_nu, k_mnc, k_buoj = ks[3:]
-                    jj = self.model.j.double()
-                    self.k_nu_f64 += self.dt * k_nu
-                    self.k_mnc_f64 += self.dt * k_mnc
-                    self.k_j_f64 -= self.dt * k_buoj * self.dt / torch.where(jj > 0, jj * jj, torch.ones_like(jj))
+                self._accumulate_exact(mode, ea.backward(grads))
                 del ea
         return misfit
+
+    def _accumulate_exact(self, mode, ks):
+        """Add exact-adjoint gradients (ExactAdjoint.backward) to the FP64
+        kernels in the reference's units (dt * dchi/dparam)."""
+        k_lam, k_mu, k_buo = ks[:3]
+        self.k_lam_f64 += self.dt * k_lam
+        self.k_mu_f64 += self.dt * k_mu
+        # buo = dt/rho: dchi/drho = -dchi/dbuo * dt / rho^2
+        rho = self.model.rho.double()
+        self.k_rho_f64 -= self.dt * k_buo * self.dt / torch.where(rho > 0, rho * rho, torch.ones_like(rho))
+        if mode == FWI_SPIN:
+            # spin: nu, mu_c and nu_c (both through mnc = mu_c + nu_c), j through dt/j
+            k_nu, k_mnc, k_buoj = ks[3:]
+            jj = self.model.j.double()
+            self.k_nu_f64 += self.dt * k_nu
+            self.k_mnc_f64 += self.dt * k_mnc
+            self.k_j_f64 -= self.dt * k_buoj * self.dt / torch.where(jj > 0, jj * jj, torch.ones_like(jj))
 
     def _free_bytes(self) -> int:
         """Free device memory including the blocks torch's caching allocator
@@ -383,13 +387,28 @@ class b200:
     def run_forward(self):
         """solver.py:166-287 for one shot set (all sources when
         combine_sources = yes, else source taskid): traces in obs_x/y/z,
-        snapshots every save_snapshot steps and output_traces files."""
+        snapshots every save_snapshot steps and output_traces files.
+
+        After setup_adjoint (adjoint_interval set) the forward also keeps
+        what run_adjoint needs for this shot, as the reference keeps
+        uy_fwd / ux_fwd / uz_fwd: the displacement snapshots of the
+        continuous adjoint (SH by default), or the checkpoints of the exact
+        adjoint (P-SV and spin by default; no save_snapshot exports then)."""
         isrc = self._isrc()
         sfe = int(self.config["save_snapshot"])
         self._fwd_batches = {}
+        self._adjoint_state, self._adj_src = {}, {}
         with self._ctx():
             for mode in self.modes:
-                b = ShotBatch(self.model, 1, self.nt, self.rec_id, tile=self.tile)
+                if self.sae and self._exact(mode):
+                    self._forward_exact_shot(mode, isrc)
+                    continue
+                snap = bool(self.sae)
+                snapv = snap and mode != FWI_SH and self.kernel_rho
+                b = ShotBatch(self.model, 1, self.nt, self.rec_id, sae=self.sae, nsa=self.nsa, snapshots=snap,
+                              snap_velocity=snapv, tile=self.tile)
+                if snap:
+                    self._adjoint_state[mode] = ("snapshots", b)
                 inj = engine.injection_lists(1, self.src_id, lambda s: isrc)
                 d = b.desc(inj=inj, stf=self._stf(mode))
                 b.clear()
@@ -415,6 +434,26 @@ class b200:
                     self.obs_z = DeviceArray(b.obs[2], None, self.stream)
                     if mode == FWI_SPIN:
                         self.obs_y = DeviceArray(b.obs[1], None, self.stream)
+        self._write_output_traces(isrc)
+        self.stream.synchronize()
+
+    def _forward_exact_shot(self, mode, isrc):
+        """Forward of one shot set with the exact adjoint's checkpoints kept."""
+        from ..adjoint import ExactAdjoint
+        ea = ExactAdjoint(self.model, self.nt, self.src_id, lambda s: isrc, 1, self._stf(mode), self.rec_id,
+                          tile=self.tile)
+        tr = ea.forward()
+        self.illum_f64 += ea.illum
+        self._adjoint_state[mode] = ("exact", ea)
+        if mode == FWI_SH:
+            self.obs_y = DeviceArray(tr[1].reshape(-1), None, self.stream)
+        else:
+            self.obs_x = DeviceArray(tr[0].reshape(-1), None, self.stream)
+            self.obs_z = DeviceArray(tr[2].reshape(-1), None, self.stream)
+            if mode == FWI_SPIN:
+                self.obs_y = DeviceArray(tr[1].reshape(-1), None, self.stream)
+
+    def _write_output_traces(self, isrc):
         if "output_traces" in self.path:
             tracedir = self.path["output_traces"]
             i = isrc if isrc >= 0 else 0
@@ -427,7 +466,6 @@ class b200:
                     comps.append(("ry", self.obs_y))
             for name, arr in comps:
                 np.save("%s/%s_%06d.npy" % (tracedir, name, i), arr.copy_to_host().reshape([self.nrec, self.nt]))
-        self.stream.synchronize()
 
     # ---------------------------------------------------------------- traces
     def import_traces(self):
@@ -521,9 +559,63 @@ class b200:
         self.stream.synchronize()
         return out
 
+    def _compute_misfit(self, comp, h_syn):
+        """fd2d.py:303-309: the L2 misfit norm of component comp ('x', 'y' or
+        'z') of the last run_forward against the observed traces h_syn, and
+        that component's adjoint source for run_adjoint -- time-reversed
+        2 taper^2 (d - s) for the continuous adjoint (waveform.py:24-34), the
+        trace gradient in forward time for the exact adjoint."""
+        c = "xyz".index(comp)
+        nrec, nt = self.nrec, self.nt
+        obs = getattr(self, "obs_" + comp).tensor.reshape(-1)
+        exact = any(k == "exact" and c in self._comps(mode) for mode, (k, _) in self._adjoint_state.items())
+        with self._ctx():
+            data = torch.as_tensor(np.ascontiguousarray(h_syn, dtype=np.float32).reshape(-1)).to(self.device)
+            src = torch.empty(nrec * nt, dtype=torch.float32, device=self.device)
+            if exact:
+                m = engine.misfit_tracegrad(data, obs, src, 1, nrec, nt, self.dt, self.stream)
+            else:
+                m = engine.misfit(data, obs, src, 1, nrec, nt, self.dt, self.stream)
+            self._adj_src[c] = src
+            misfit = float(m.sum().item())
+        return misfit
+
+    @staticmethod
+    def _comps(mode):
+        """Component slots whose traces enter the misfit of a wave type."""
+        return (1,) if mode == FWI_SH else (0, 2)
+
     def run_adjoint(self):
-        """solver.py:290-329 for the batch of the last run_kernel chunk."""
-        raise NotImplementedError("run_adjoint is driven by run_kernel, which batches every shot")
+        """solver.py:290-321 for the shot of the last run_forward, after
+        _compute_misfit of its components: the adjoint run whose kernels are
+        added to k_mu (and k_lam, k_rho) -- the snapshot-correlation adjoint
+        of the reference for SH, the exact transposed step for P-SV and spin
+        (the reference's P-SV branch cannot run, solver.py:324-329)."""
+        state = getattr(self, "_adjoint_state", None)
+        if not state:
+            raise RuntimeError("run_adjoint needs setup_adjoint, then run_forward")
+        nrec, nt = self.nrec, self.nt
+        with self._ctx():
+            for mode, (kind, obj) in state.items():
+                comps = self._comps(mode)
+                missing = [c for c in comps if c not in self._adj_src]
+                if missing:
+                    raise RuntimeError("run_adjoint: _compute_misfit('%s') first" % "xyz"[missing[0]])
+                if kind == "exact":
+                    grads = [self._adj_src[c].view(1, nrec, nt) if c in comps else None for c in range(3)]
+                    self._accumulate_exact(mode, obj.backward(grads))
+                else:
+                    b = obj
+                    adstf = [self._adj_src.get(c) if c in comps else None for c in range(3)]
+                    snapv = mode != FWI_SH and self.kernel_rho
+                    kern = (None, self.k_mu_f64, None) if mode == FWI_SH else \
+                        (self.k_lam_f64, self.k_mu_f64, self.k_rho_f64 if snapv else None)
+                    d = b.desc(inj=engine.adjoint_injection_lists(1, self.rec_id), stf=adstf, record=False,
+                               kernels=kern)
+                    b.clear()
+                    b.run(d, True, 0, nt)
+        self._adjoint_state, self._adj_src = {}, {}
+        self._illum_valid = all(self._exact(m) for m in self.modes)
 
     def run_kernel(self, adj):
         """solver.py:332-404, all shots of this process batched: forward with
@@ -556,8 +648,6 @@ class b200:
                         m = engine.misfit(data, b.obs[c], adstf[c], n, nrec, nt, self.dt)
                         misfit += float(m.sum().item())
                     if adj:
-                        if mode == FWI_SPIN:
-                            raise NotImplementedError("the spin adjoint is not provided")
                         kern = (None, self.k_mu_f64, None) if mode == FWI_SH else \
                                (self.k_lam_f64, self.k_mu_f64, self.k_rho_f64 if snapv else None)
                         d = b.desc(inj=engine.adjoint_injection_lists(n, self.rec_id), stf=adstf, record=False,
