@@ -163,7 +163,7 @@ def _medium_case(mode, seed, nx=83, nz=70, nt=300, nsrc=3, nrec=9):
                       vs=(1732 + 200 * rng.uniform(-1, 1, n)).astype(np.float32),
                       rho=(2600 + 200 * rng.uniform(-1, 1, n)).astype(np.float32))
     f0 = 10.0 if mode != "spin" else 60.0
-    src = np.array([[rng.uniform(3, nx - 4) * h, rng.uniform(3, nz - 4) * h, 0, f0, 1.2 / f0,
+    src = np.array([[rng.uniform(3, max(4, nx - 4)) * h, rng.uniform(3, max(4, nz - 4)) * h, 0, f0, 1.2 / f0,
                      rng.uniform(-90, 90), 1e10] for _ in range(nsrc)])
     # receivers include the grid's edge rows and columns
     rec = np.array([[0, 0], [(nx - 1) * h, (nz - 1) * h], [0, (nz - 1) * h], [(nx - 1) * h, 5 * h]] +
