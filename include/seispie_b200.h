@@ -118,6 +118,9 @@ typedef struct fwi_batch {
      * rec_cell[rec_order[i]] non-decreasing.  Required by displacement-free
      * forward runs that record traces (see fwi_run). */
     const int *rec_order;
+    /* Displacement-free batches: row slots of the row-marching kernel's
+     * staging ring, 3, 4, 6 or 8 (0 = chosen from the row length). */
+    int ring;
 } fwi_batch;
 
 /* ABI version of the loaded library (FWI_ABI_VERSION). */

@@ -114,6 +114,8 @@ static int check_batch(const fwi_batch *b, int adjoint, int it0, int nsteps) {
             REQUIRE(!b->snap_u[c] && !b->snap_v[c], "displacement-free batches take no snapshots");
         const bool rec = b->nrec > 0 && (b->obs[0] || b->obs[1] || b->obs[2]);
         REQUIRE(!rec || b->rec_order, "displacement-free batches that record traces need rec_order");
+        REQUIRE(b->ring == 0 || b->ring == 3 || b->ring == 4 || b->ring == 6 || b->ring == 8,
+                "ring must be 0, 3, 4, 6 or 8 (got %d)", b->ring);
     }
     if (adjoint) {
         REQUIRE(b->sae >= 1, "the adjoint needs adjoint_interval >= 1");

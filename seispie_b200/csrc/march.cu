@@ -84,7 +84,8 @@ struct MarchArgs {
 
 // Shared-memory layout, in floats: ring [nslots][NF][rl], velocity ring
 // [kVRing][NV][rl], injection window (cells, NINJ value rows), receiver
-// window (cells, ids), two cursors, then the mbarriers (8-byte aligned).
+// window (cells, ids), two double-buffered cursors, then the mbarriers
+// (8-byte aligned).
 struct MarchLayout {
     int vring, icell, ival, rcell, rid, cur, bar;
     size_t bytes;
@@ -97,8 +98,8 @@ __host__ __device__ inline MarchLayout march_layout(int nf, int nv, int ninj, in
     L.ival = L.icell + kPts;
     L.rcell = L.ival + ninj * kPts;
     L.rid = L.rcell + kPts;
-    L.cur = L.rid + kPts;  // two cursors (8 ints)
-    L.bar = (L.cur + 8 + 1) / 2 * 2;
+    L.cur = L.rid + kPts;  // two double-buffered cursors (16 ints)
+    L.bar = (L.cur + 16 + 1) / 2 * 2;
     L.bytes = sizeof(float) * (size_t)L.bar + 8 * (size_t)nslots;
     return L;
 }
@@ -157,7 +158,8 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
     float *const i_val = smem + L.ival;
     int *const r_cell = reinterpret_cast<int *>(smem + L.rcell);
     int *const r_id = reinterpret_cast<int *>(smem + L.rid);
-    Cursor *const cur_s = reinterpret_cast<Cursor *>(smem + L.cur);  // [0] injection, [1] receivers
+    // cursors [list][buffer]: list 0 injection, 1 receivers; the buffer in use flips at every store
+    Cursor *const cur_s = reinterpret_cast<Cursor *>(smem + L.cur);
     uint64_t *const full = reinterpret_cast<uint64_t *>(smem + L.bar);
 
     const int tid = threadIdx.x, j0 = 4 * tid;
@@ -223,17 +225,18 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
         c.wn = n;
         __syncthreads();
     };
-    // after the points of a row: store the cursor back (block-wide) and
-    // return the cell of the next point, or kNone
-    auto park = [&](Cursor &c, int which, bool inj) -> int {
+    // after the points of a row: store the cursor into the other buffer of
+    // its list (slow threads may still read the one in use; the row barrier
+    // that follows orders the store before the next use) and return the cell
+    // of the next point, or kNone.  Every thread holds the same cursor.
+    auto park = [&](Cursor &c, int which, int &buf, bool inj) -> int {
         if (c.p < c.end && c.p - c.w0 >= c.wn) {
             if (inj) load_inj(c);
             else load_rec(c);
         }
         const int nxt = c.p < c.end ? (inj ? i_cell : r_cell)[c.p - c.w0] : kNone;
-        __syncthreads();
-        if (tid == 0) cur_s[which] = c;
-        __syncthreads();
+        buf ^= 1;
+        if (tid == 0) cur_s[2 * which + buf] = c;
         return nxt;
     };
     // model row `row` at this thread's columns (zero outside the grid)
@@ -268,15 +271,16 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
             const int r0 = rec_on ? lower_bound_cells(a.rec_cell, a.rec_order, 0, a.nrec, a0 * nz) : 0;
             const int r1 = rec_on ? lower_bound_cells(a.rec_cell, a.rec_order, 0, a.nrec, b0 * nz) : 0;
             cur_s[0] = Cursor{i0, i1, i0, 0};
-            cur_s[1] = Cursor{r0, r1, r0, 0};
+            cur_s[2] = Cursor{r0, r1, r0, 0};
         }
         __syncthreads();
         int inj_next, rec_next;  // cell of the next injection entry / receiver, or kNone
+        int ib = 0, rb = 0;      // cursor buffers in use
         {
             Cursor c = cur_s[0];
-            inj_next = c.p < c.end ? park(c, 0, true) : kNone;
-            c = cur_s[1];
-            rec_next = c.p < c.end ? park(c, 1, false) : kNone;
+            inj_next = c.p < c.end ? park(c, 0, ib, true) : kNone;
+            c = cur_s[2];
+            rec_next = c.p < c.end ? park(c, 1, rb, false) : kNone;
         }
 
         bool ok = true;
@@ -386,7 +390,7 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
                     for (int q = 0; q < NINJ; q++)
 #pragma unroll
                         for (int e = 0; e < 4; e++) acc[q][e] = 0.f;
-                    Cursor c = cur_s[0];
+                    Cursor c = cur_s[ib];
                     while (c.p < c.end) {
                         if (c.p - c.w0 >= c.wn) load_inj(c);
                         const int k = c.p - c.w0, cell = i_cell[k];
@@ -400,7 +404,7 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
                             }
                         c.p++;
                     }
-                    inj_next = park(c, 0, true);
+                    inj_next = park(c, 0, ib, true);
 #pragma unroll
                     for (int q = 0; q < NV; q++)
 #pragma unroll
@@ -426,7 +430,7 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
                 // receivers of row r record the new velocity (save_obs, solver.py:151-156)
                 if (rec_next < (r + 1) * nz) {
                     const int lo = r * nz, hi = lo + nz;
-                    Cursor c = cur_s[1];
+                    Cursor c = cur_s[2 + rb];
                     while (c.p < c.end) {
                         if (c.p - c.w0 >= c.wn) load_rec(c);
                         const int k = c.p - c.w0, cell = r_cell[k];
@@ -444,7 +448,7 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
                         }
                         c.p++;
                     }
-                    rec_next = park(c, 1, false);
+                    rec_next = park(c, 1, rb, false);
                 }
             } else {
 #pragma unroll
@@ -570,11 +574,16 @@ __global__ void displacement_traces_kernel(float *obs, long long ntr, int nt, in
 
 static int comp_slot_of(int mode, int q) { return mode == FWI_SH ? 1 : (q == 0 ? 0 : 2); }
 
-// Ring depth for a row length: 8 slots while two CTAs fit an SM, else 4
-// while two fit, else 8 with one CTA per SM.
-static int march_slots(int mode, int rl, size_t *bytes) {
+// Ring depth for a row length: the requested depth (3, 4, 6 or 8), or by
+// default 8 slots while two CTAs fit an SM, else 4 while two fit, else 8
+// with one CTA per SM.  0 if it does not fit.
+static int march_slots(int mode, int rl, int want, size_t *bytes) {
     const int nf = mode == FWI_SH ? 3 : 5, nv = mode == FWI_SH ? 1 : 2, ninj = mode == FWI_SH ? 1 : 2;
     const size_t two = (size_t)110 * 1024, one = (size_t)224 * 1024;
+    if (want) {
+        *bytes = march_layout(nf, nv, ninj, rl, want).bytes;
+        return *bytes <= one ? want : 0;
+    }
     const size_t b8 = march_layout(nf, nv, ninj, rl, 8).bytes, b4 = march_layout(nf, nv, ninj, rl, 4).bytes;
     if (b8 <= two || (b4 > two && b8 <= one)) {
         *bytes = b8;
@@ -671,11 +680,22 @@ int launch_march(const fwi_batch *b, int it, cudaStream_t st) {
     const int nthr = ((b->pitch / 4 + 31) / 32) * 32;
     a.rl = 4 * nthr + 8;
     size_t bytes = 0;
-    const int n = march_slots(mode, a.rl, &bytes);
+    const int n = march_slots(mode, a.rl, b->ring, &bytes);
     if (!n) return set_error(FWI_ERANGE, "row-marching step: rows of %d columns do not fit shared memory", b->pitch);
-    if (mode == FWI_SH)
-        return n == 8 ? launch_march_mode<FWI_SH, 8>(a, nthr, bytes, st) : launch_march_mode<FWI_SH, 4>(a, nthr, bytes, st);
-    return n == 8 ? launch_march_mode<FWI_PSV, 8>(a, nthr, bytes, st) : launch_march_mode<FWI_PSV, 4>(a, nthr, bytes, st);
+    if (mode == FWI_SH) {
+        switch (n) {
+            case 3: return launch_march_mode<FWI_SH, 3>(a, nthr, bytes, st);
+            case 4: return launch_march_mode<FWI_SH, 4>(a, nthr, bytes, st);
+            case 6: return launch_march_mode<FWI_SH, 6>(a, nthr, bytes, st);
+            default: return launch_march_mode<FWI_SH, 8>(a, nthr, bytes, st);
+        }
+    }
+    switch (n) {
+        case 3: return launch_march_mode<FWI_PSV, 3>(a, nthr, bytes, st);
+        case 4: return launch_march_mode<FWI_PSV, 4>(a, nthr, bytes, st);
+        case 6: return launch_march_mode<FWI_PSV, 6>(a, nthr, bytes, st);
+        default: return launch_march_mode<FWI_PSV, 8>(a, nthr, bytes, st);
+    }
 }
 
 // Binary version (major*10 + minor) of the device code the library loaded.

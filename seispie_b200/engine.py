@@ -204,6 +204,7 @@ class ShotBatch:
                         self.snap_v[c] = z(nsa, *shape)
         self.cur = 0
         self.tile = int(tile)
+        self.ring = 0  # staging-ring depth of the row-marching kernel (0 = automatic)
 
     # ------------------------------------------------------------ descriptors
     def desc(self, inj=None, stf=(None, None, None), record=True, kernels=(None, None, None)) -> FwiBatch:
@@ -212,7 +213,7 @@ class ShotBatch:
         b = FwiBatch()
         b.mode, b.nx, b.nz, b.pitch = self.mode, g.nx, g.nz, g.pitch
         b.nshots, b.nt, b.dx, b.dz, b.dt = self.nshots, self.nt, float(g.dx), float(g.dz), float(m.dt)
-        b.cur, b.tile = self.cur, self.tile
+        b.cur, b.tile, b.ring = self.cur, self.tile, self.ring
         for h in range(2):
             for f, t in enumerate(self.sig[h]):
                 b.sig[h][f] = ptr(t)
