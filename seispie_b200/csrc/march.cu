@@ -59,9 +59,9 @@ int march_device_status(int clear, int *status) {
     return 0;
 }
 
-constexpr int kPts = 256;        // points (injection entries, receivers) staged per window
+constexpr int kPts = 128;        // points (injection entries, receivers) staged per window
 constexpr int kMaxPitch = 1024;  // row length (floats) a CTA can span: 256 threads of 4 columns
-constexpr int kVRing = 8;        // rows of the new-velocity ring
+constexpr int kVRing = 5;        // rows of the new-velocity ring (rows s-1 .. s+2 live, plus one for barrier slack)
 
 struct MarchArgs {
     int nx, nz, pitch, nt, it, nrec;
@@ -169,7 +169,10 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
     const uint32_t row_bytes = 4u * (uint32_t)pitch;
     // row buffers start 4 floats into their slot so that columns -4 .. rl-5 are addressable
     auto ring_row = [&](int slot, int f) -> float * { return smem + (slot * NF + f) * RL + 4; };
-    auto vel_row = [&](int row, int c) -> float * { return smem + L.vring + ((row & (kVRing - 1)) * NV + c) * RL + 4; };
+    // row >= -1 (the row above the grid is only read where D+x is masked)
+    auto vel_row = [&](int row, int c) -> float * {
+        return smem + L.vring + (((row + kVRing) % kVRing) * NV + c) * RL + 4;
+    };
 
     if (tid == 0) {
         for (int i = 0; i < N; i++) mbar_init(&full[i], 1);
@@ -189,6 +192,20 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
         for (int c = 0; c < NV; c++) bulk_load(ring_row(slot, NS + c), a.vel_in[c] + o, row_bytes, &full[slot]);
     };
     auto wait_seq = [&](int sn) -> bool { return mbar_wait(&full[sn % N], (uint32_t)((sn / N) & 1)); };
+    // Only warp 0 waits for rows (the others wait at the block barrier that
+    // follows, without issuing); the barrier then makes the landed row
+    // visible to every thread.
+    const bool waiter = tid < 32;
+    // per-column masks, fixed for the whole march: D-z (2 <= j < nz-2),
+    // D+z (1 <= j < nz-2) and "inside the grid" (j < nz)
+    bool zm[4], zp[4], zin[4];
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        const int c = j0 + e;
+        zm[e] = c >= 2 && c < nz - 2;
+        zp[e] = c >= 1 && c < nz - 2;
+        zin[e] = c < nz;
+    }
 
     const bool rec_on = a.rec_order && a.nrec > 0 && (a.obs[0] || (NV > 1 && a.obs[1]));
     const bool inj_on = a.inj_ptr != nullptr;
@@ -288,11 +305,14 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
         // r-2 .. r+1 (SH: sxy; P-SV: sxx, sxz), the other stress field at rows
         // r-2 .. r (SH: szy; P-SV: szz)
         float wx[NW][4][4], wz[3][4];
+        // the window rows va-2 .. va must have landed before the first iteration
+        if (waiter)
+            for (int q = qa; q <= va; q++) ok = wait_seq(sb + q) && ok;
+        if (__syncthreads_or(!ok)) goto bail;
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             const int q = va - 2 + k;
             if (q >= qa) {
-                ok = wait_seq(sb + q) && ok;
                 const int sl = (sb + q) % N;
                 ld4(wx[0][k], ring_row(sl, FX0) + j0);
                 if (NW > 1) ld4(wx[NW - 1][k], ring_row(sl, FX1) + j0);
@@ -311,13 +331,17 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
         ld_model(bnd, a.bound, va);
         ld_model(ip0, a.ip[0], va - 2);
         if (MODE == FWI_PSV) ld_model(ip1, a.ip[1], va - 2);
-        if (__syncthreads_or(!ok)) goto bail;
-        // rows above va are consumed: their slots take the next rows
+        // rows above va are consumed once every thread has its window: their
+        // slots take the next rows; then row va+1, which the first iteration
+        // reads, has to land
+        __syncthreads();
         for (int q = qa; q < va; q++)
             if (nexti < qb) {
                 if (tid == 0) issue(soff, nexti, sb + nexti);
                 nexti++;
             }
+        if (waiter && va + 1 < qb) ok = wait_seq(sb + va + 1) && ok;
+        if (__syncthreads_or(!ok)) goto bail;
 
         for (int r = va; r < b0 + 2; r++) {
             // next iteration's model values (one row ahead)
@@ -336,8 +360,7 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
             const long long grow = soff + (long long)r * pitch + j0;
             if (r < vb) {
                 // ---- velocity of row r
-                if (r + 1 < qb) {
-                    ok = wait_seq(sb + r + 1) && ok;
+                if (r + 1 < qb) {  // landed: waited for before the previous row's barrier
                     const int sl = (sb + r + 1) % N;
                     ld4(wx[0][3], ring_row(sl, FX0) + j0);
                     if (NW > 1) ld4(wx[NW - 1][3], ring_row(sl, FX1) + j0);
@@ -362,8 +385,7 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
 #pragma unroll
                     for (int e = 0; e < 4; e++) {
                         const int c = j0 + e;
-                        const bool okz = c >= 2 && c < nz - 2;
-                        out[e] = okz ? cz1 * (x[e + 2] - x[e + 1]) - cz2 * (x[e + 3] - x[e]) : 0.f;
+                        out[e] = zm[e] ? cz1 * (x[e + 2] - x[e + 1]) - cz2 * (x[e + 3] - x[e]) : 0.f;
                     }
                 };
                 float ds[NV][4];
@@ -418,8 +440,8 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
 #pragma unroll
                     for (int e = 0; e < 4; e++) {
                         const float v = bnd[e] * (vold[e] + ds[c][e] * buo[e]);
-                        vn[c][e] = j0 + e < nz ? v : 0.f;  // padding columns stay zero
-                        if (j0 + e >= nz) ds[c][e] = 0.f;
+                        vn[c][e] = zin[e] ? v : 0.f;  // padding columns stay zero
+                        if (!zin[e]) ds[c][e] = 0.f;
                     }
                     st4(vel_row(r, c) + j0, vn[c]);
                     if (own) {
@@ -458,6 +480,8 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
                     st4(vel_row(r, c) + j0, vn[c]);
                 }
             }
+            // the next iteration reads row r+2: warp 0 waits for it before the barrier
+            if (waiter && r + 2 < qb && r + 2 < vb + 1) ok = wait_seq(sb + r + 2) && ok;
             if (__syncthreads_or(!ok)) goto bail;
             // row r is consumed: its slot takes row r + N
             if (nexti < qb) {
@@ -487,9 +511,8 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
 #pragma unroll
                     for (int e = 0; e < 4; e++) {
                         const int cc = j0 + e;
-                        const bool okz = cc >= 1 && cc < nz - 2;
                         ex[c][e] = okx ? cx1 * (v2[e] - v1[e]) - cx2 * (v3[e] - v0[e]) : 0.f;
-                        ez[c][e] = okz ? cz1 * (y[e + 2] - y[e + 1]) - cz2 * (y[e + 3] - y[e]) : 0.f;
+                        ez[c][e] = zp[e] ? cz1 * (y[e + 2] - y[e + 1]) - cz2 * (y[e + 3] - y[e]) : 0.f;
                     }
                 }
                 if constexpr (MODE == FWI_SH) {
@@ -497,7 +520,7 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
 #pragma unroll
                     for (int e = 0; e < 4; e++) {
                         const float dm = dt * ip0[e], exy = ex[0][e], ezy = ez[0][e];
-                        const bool in = j0 + e < nz;  // padding columns stay zero
+                        const bool in = zin[e];  // padding columns stay zero
                         o0[e] = in ? wx[0][0][e] + dm * exy : 0.f;
                         o1[e] = in ? wz[0][e] + dm * ezy : 0.f;
                     }
@@ -514,7 +537,7 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
                         const float lam = ip0[e], mu = ip1[e];
                         const float vxx = ex[0][e], vxz = ez[0][e], vzx = ex[1][e], vzz = ez[1][e];
                         const float l2m = lam + 2.f * mu, shear = vxz + vzx;
-                        const bool in = j0 + e < nz;  // padding columns stay zero
+                        const bool in = zin[e];  // padding columns stay zero
                         o0[e] = in ? wx[0][0][e] + dt * (l2m * vxx + lam * vzz) : 0.f;
                         o1[e] = in ? wz[0][e] + dt * (l2m * vzz + lam * vxx) : 0.f;
                         o2[e] = in ? wx[1][0][e] + dt * (mu * shear) : 0.f;
@@ -575,25 +598,29 @@ __global__ void displacement_traces_kernel(float *obs, long long ntr, int nt, in
 static int comp_slot_of(int mode, int q) { return mode == FWI_SH ? 1 : (q == 0 ? 0 : 2); }
 
 // Ring depth for a row length: the requested depth (3, 4, 6 or 8), or by
-// default 8 slots while two CTAs fit an SM, else 4 while two fit, else 8
-// with one CTA per SM.  0 if it does not fit.
+// default the depth that lets the most CTAs share an SM (228 KB of shared
+// memory, 1 KB of it reserved per CTA), the deepest among those.  0 if it
+// does not fit.
 static int march_slots(int mode, int rl, int want, size_t *bytes) {
     const int nf = mode == FWI_SH ? 3 : 5, nv = mode == FWI_SH ? 1 : 2, ninj = mode == FWI_SH ? 1 : 2;
-    const size_t two = (size_t)110 * 1024, one = (size_t)224 * 1024;
+    const size_t sm = (size_t)228 * 1024, cap = (size_t)227 * 1024;
     if (want) {
         *bytes = march_layout(nf, nv, ninj, rl, want).bytes;
-        return *bytes <= one ? want : 0;
+        return *bytes <= cap ? want : 0;
     }
-    const size_t b8 = march_layout(nf, nv, ninj, rl, 8).bytes, b4 = march_layout(nf, nv, ninj, rl, 4).bytes;
-    if (b8 <= two || (b4 > two && b8 <= one)) {
-        *bytes = b8;
-        return 8;
+    int best = 0;
+    size_t best_ctas = 0;
+    for (int n : {3, 4, 6, 8}) {
+        const size_t b = march_layout(nf, nv, ninj, rl, n).bytes;
+        if (b > cap) continue;
+        const size_t ctas = sm / (b + 1024);
+        if (ctas >= best_ctas) {
+            best_ctas = ctas;
+            best = n;
+            *bytes = b;
+        }
     }
-    if (b4 <= one) {
-        *bytes = b4;
-        return 4;
-    }
-    return 0;
+    return best;
 }
 
 bool march_supported(const fwi_batch *b) {
