@@ -37,6 +37,7 @@
 //     by cell.  Each CTA stages the points of its rows in shared-memory
 //     windows and walks them with the march.
 #include <cstdio>
+#include <type_traits>
 
 #include "common.cuh"
 #include "stencil.cuh"
@@ -206,6 +207,8 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
         zp[e] = c >= 1 && c < nz - 2;
         zin[e] = c < nz;
     }
+    // warps without a masked column (all but those at the z edges) skip the masks
+    const bool zedge = __any_sync(0xffffffffu, !(j0 >= 2 && j0 + 3 < nz - 2));
 
     const bool rec_on = a.rec_order && a.nrec > 0 && (a.obs[0] || (NV > 1 && a.obs[1]));
     const bool inj_on = a.inj_ptr != nullptr;
@@ -375,35 +378,41 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
                 auto dxm = [&](int w, int e) -> float {
                     return okx ? cx1 * (wx[w][2][e] - wx[w][1][e]) - cx2 * (wx[w][3][e] - wx[w][0][e]) : 0.f;
                 };
-                // D-z of stress field f at row r, element e, from columns j0-2 .. j0+4:
-                // x[i] = column j0-2+i, with the centre taken from `cen`
-                auto dzm_row = [&](int f, const float (&cen)[4], float (&out)[4]) {
-                    const float *s = ring_row(sr, f) + j0;
-                    const float2 l2 = *reinterpret_cast<const float2 *>(s - 2);
-                    const float rr = s[4];
-                    const float x[7] = {l2.x, l2.y, cen[0], cen[1], cen[2], cen[3], rr};
+                float ds[NV][4];
+                // the stress divergence; ZE: this warp holds columns near a z edge (per-column masks)
+                auto divergence = [&](auto ze_t) {
+                    constexpr bool ZE = decltype(ze_t)::value;
+                    // D-z of stress field f at row r, element e, from columns j0-2 .. j0+4:
+                    // x[i] = column j0-2+i, with the centre taken from `cen`
+                    auto dzm_row = [&](int f, const float (&cen)[4], float (&out)[4]) {
+                        const float *s = ring_row(sr, f) + j0;
+                        const float2 l2 = *reinterpret_cast<const float2 *>(s - 2);
+                        const float rr = s[4];
+                        const float x[7] = {l2.x, l2.y, cen[0], cen[1], cen[2], cen[3], rr};
 #pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        const int c = j0 + e;
-                        out[e] = zm[e] ? cz1 * (x[e + 2] - x[e + 1]) - cz2 * (x[e + 3] - x[e]) : 0.f;
+                        for (int e = 0; e < 4; e++) {
+                            const float d = cz1 * (x[e + 2] - x[e + 1]) - cz2 * (x[e + 3] - x[e]);
+                            out[e] = (!ZE || zm[e]) ? d : 0.f;
+                        }
+                    };
+                    if constexpr (MODE == FWI_SH) {
+                        float zz[4];
+                        dzm_row(1, wz[2], zz);
+#pragma unroll
+                        for (int e = 0; e < 4; e++) ds[0][e] = dxm(0, e) + zz[e];
+                    } else {
+                        float zxz[4], zzz[4];
+                        dzm_row(2, wx[1][2], zxz);
+                        dzm_row(1, wz[2], zzz);
+#pragma unroll
+                        for (int e = 0; e < 4; e++) {
+                            ds[0][e] = dxm(0, e) + zxz[e];
+                            ds[1][e] = dxm(1, e) + zzz[e];
+                        }
                     }
                 };
-                float ds[NV][4];
-                if constexpr (MODE == FWI_SH) {
-                    float zm[4];
-                    dzm_row(1, wz[2], zm);
-#pragma unroll
-                    for (int e = 0; e < 4; e++) ds[0][e] = dxm(0, e) + zm[e];
-                } else {
-                    float zxz[4], zzz[4];
-                    dzm_row(2, wx[1][2], zxz);
-                    dzm_row(1, wz[2], zzz);
-#pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        ds[0][e] = dxm(0, e) + zxz[e];
-                        ds[1][e] = dxm(1, e) + zzz[e];
-                    }
-                }
+                if (zedge) divergence(std::true_type{});
+                else divergence(std::false_type{});
                 // sources of row r, summed per cell in entry order (stf_dsy / stf_dsxz, solver.py:78-93)
                 if (inj_next < (r + 1) * nz) {
                     const int lo = r * nz, hi = lo + nz;
@@ -433,22 +442,27 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
                         for (int e = 0; e < 4; e++) ds[q][e] += acc[q][e];
                 }
                 const bool own = r >= a0 && r < b0 && tin;
+                auto velocity = [&](auto ze_t) {
+                    constexpr bool ZE = decltype(ze_t)::value;
 #pragma unroll
-                for (int c = 0; c < NV; c++) {
-                    float vold[4];
-                    ld4(vold, ring_row(sr, NS + c) + j0);
+                    for (int c = 0; c < NV; c++) {
+                        float vold[4];
+                        ld4(vold, ring_row(sr, NS + c) + j0);
 #pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        const float v = bnd[e] * (vold[e] + ds[c][e] * buo[e]);
-                        vn[c][e] = zin[e] ? v : 0.f;  // padding columns stay zero
-                        if (!zin[e]) ds[c][e] = 0.f;
+                        for (int e = 0; e < 4; e++) {
+                            const float v = bnd[e] * (vold[e] + ds[c][e] * buo[e]);
+                            vn[c][e] = (!ZE || zin[e]) ? v : 0.f;  // padding columns stay zero
+                            if (ZE && !zin[e]) ds[c][e] = 0.f;
+                        }
+                        st4(vel_row(r, c) + j0, vn[c]);
+                        if (own) {
+                            st4(a.vel_out[c] + grow, vn[c]);
+                            if (a.seg_ds[c]) st4(a.seg_ds[c] + grow, ds[c]);
+                        }
                     }
-                    st4(vel_row(r, c) + j0, vn[c]);
-                    if (own) {
-                        st4(a.vel_out[c] + grow, vn[c]);
-                        if (a.seg_ds[c]) st4(a.seg_ds[c] + grow, ds[c]);
-                    }
-                }
+                };
+                if (zedge) velocity(std::true_type{});
+                else velocity(std::false_type{});
                 // receivers of row r record the new velocity (save_obs, solver.py:151-156)
                 if (rec_next < (r + 1) * nz) {
                     const int lo = r * nz, hi = lo + nz;
@@ -491,7 +505,8 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
 
             // ---- stress of row s = r - 2 (add_sy / add_sxz, solver.py:128-149)
             const int s = r - 2;
-            if (s >= a0 && s < b0 && tin) {
+            auto stress = [&](auto ze_t) {
+                constexpr bool ZE = decltype(ze_t)::value;
                 const bool okx = s >= 1 && s < nx - 2;
                 const long long gs = soff + (long long)s * pitch + j0;
                 float ex[NV][4], ez[NV][4];
@@ -510,9 +525,9 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
                     const float y[7] = {l1, v1[0], v1[1], v1[2], v1[3], r2.x, r2.y};
 #pragma unroll
                     for (int e = 0; e < 4; e++) {
-                        const int cc = j0 + e;
                         ex[c][e] = okx ? cx1 * (v2[e] - v1[e]) - cx2 * (v3[e] - v0[e]) : 0.f;
-                        ez[c][e] = zp[e] ? cz1 * (y[e + 2] - y[e + 1]) - cz2 * (y[e + 3] - y[e]) : 0.f;
+                        const float d = cz1 * (y[e + 2] - y[e + 1]) - cz2 * (y[e + 3] - y[e]);
+                        ez[c][e] = (!ZE || zp[e]) ? d : 0.f;
                     }
                 }
                 if constexpr (MODE == FWI_SH) {
@@ -520,7 +535,7 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
 #pragma unroll
                     for (int e = 0; e < 4; e++) {
                         const float dm = dt * ip0[e], exy = ex[0][e], ezy = ez[0][e];
-                        const bool in = zin[e];  // padding columns stay zero
+                        const bool in = !ZE || zin[e];  // padding columns stay zero
                         o0[e] = in ? wx[0][0][e] + dm * exy : 0.f;
                         o1[e] = in ? wz[0][e] + dm * ezy : 0.f;
                     }
@@ -537,7 +552,7 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
                         const float lam = ip0[e], mu = ip1[e];
                         const float vxx = ex[0][e], vxz = ez[0][e], vzx = ex[1][e], vzz = ez[1][e];
                         const float l2m = lam + 2.f * mu, shear = vxz + vzx;
-                        const bool in = zin[e];  // padding columns stay zero
+                        const bool in = !ZE || zin[e];  // padding columns stay zero
                         o0[e] = in ? wx[0][0][e] + dt * (l2m * vxx + lam * vzz) : 0.f;
                         o1[e] = in ? wz[0][e] + dt * (l2m * vzz + lam * vxx) : 0.f;
                         o2[e] = in ? wx[1][0][e] + dt * (mu * shear) : 0.f;
@@ -552,6 +567,10 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
                         st4(a.seg_e[2] + gs, sh);
                     }
                 }
+            };
+            if (s >= a0 && s < b0 && tin) {
+                if (zedge) stress(std::true_type{});
+                else stress(std::false_type{});
             }
 #pragma unroll
             for (int w = 0; w < NW; w++)
