@@ -266,10 +266,13 @@ def main():
     ev = {}
     if a.gradient == "exact":
         # exact discrete adjoint with checkpointed recomputation (the P-SV gradient of the solver)
-        from seispie_b200.adjoint import ExactAdjoint
-        # per-step stores of the last steps kept from the forward sweep in half of the free HBM
+        from seispie_b200._lib import FWI_PSV
+        from seispie_b200.adjoint import ExactAdjoint, max_tail_bytes
+        # per-step stores of the last steps kept from the forward sweep: the longest tail that fits
+        # 90 % of the free HBM with the checkpoints, segment stores, wavefields and traces
         free, _ = torch.cuda.mem_get_info(dev)
-        ea = ExactAdjoint(m_init, nt, sid, lambda s: s, nshots, stf, rid, tile=a.tile, tail_memory=0.5 * free)
+        tail = max_tail_bytes(nt, FWI_PSV, nshots, m_init.grid, 0.9 * free, a.nrec)
+        ea = ExactAdjoint(m_init, nt, sid, lambda s: s, nshots, stf, rid, tile=a.tile, tail_memory=tail)
         checkpointing = {"segment": ea.K, "checkpoints": ea.nseg, "stored_tail_steps": ea.tail}
         grads = [torch.empty((nshots, a.nrec, nt), dtype=torch.float32, device=dev) if c != 1 else None
                  for c in range(3)]

@@ -68,6 +68,35 @@ def fixed_bytes(nt: int, mode: int, nshots: int, grid: Grid, nrec: int = 0, segm
     return (math.ceil(nt / k) * state + k * per_step + 2 * batch) * field + 3 * 4 * nshots * nrec * nt * NV[mode]
 
 
+def max_tail_bytes(nt: int, mode: int, nshots: int, grid: Grid, budget_bytes: float, nrec: int = 0,
+                   segment: int | None = None) -> int:
+    """Largest stored tail (as ExactAdjoint's tail_memory, in bytes) whose
+    ExactAdjoint (levels = 1) fits budget_bytes in all: checkpoints of the
+    steps before the tail, one segment of per-step stores, the tail's
+    per-step stores, both batches' wavefields and the trace arrays (the
+    terms of fixed_bytes).  A longer tail needs fewer checkpoints."""
+    k = segment or default_segment(nt, mode, nshots, grid)
+    field = 4 * nshots * grid.nx * grid.pitch
+    state = state_fields(mode, grid)
+    per_step = strain_fields(mode) + NV[mode]
+    batch = 2 * NS[mode] + 2 * NV[mode] + (state - NS[mode] - NV[mode])
+    traces = 3 * 4 * nshots * nrec * nt * NV[mode]
+
+    def need(t):
+        return (math.ceil((nt - t) / k) * state + k * per_step + t * per_step + 2 * batch) * field + traces
+
+    lo, hi = 0, nt  # need() grows with t: the largest t with need(t) <= budget
+    if need(0) > budget_bytes:
+        return 0
+    while lo < hi:
+        mid = (lo + hi + 1) // 2
+        if need(mid) <= budget_bytes:
+            lo = mid
+        else:
+            hi = mid - 1
+    return lo * per_step * field
+
+
 def two_level_segments(nt: int, mode: int) -> tuple:
     """(K1, K2) minimising the memory of two-level checkpointing,
     nt/K1 + K1/K2 checkpoints of S = NS+2NV fields plus K2 steps of

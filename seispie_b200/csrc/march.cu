@@ -170,10 +170,7 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
     const uint32_t row_bytes = 4u * (uint32_t)pitch;
     // row buffers start 4 floats into their slot so that columns -4 .. rl-5 are addressable
     auto ring_row = [&](int slot, int f) -> float * { return smem + (slot * NF + f) * RL + 4; };
-    // row >= -1 (the row above the grid is only read where D+x is masked)
-    auto vel_row = [&](int row, int c) -> float * {
-        return smem + L.vring + (((row + kVRing) % kVRing) * NV + c) * RL + 4;
-    };
+
 
     if (tid == 0) {
         for (int i = 0; i < N; i++) mbar_init(&full[i], 1);
@@ -346,13 +343,33 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
         if (waiter && va + 1 < qb) ok = wait_seq(sb + va + 1) && ok;
         if (__syncthreads_or(!ok)) goto bail;
 
-        for (int r = va; r < b0 + 2; r++) {
-            // next iteration's model values (one row ahead)
+        // vk: velocity-ring slot of row r
+        for (int r = va, vk = va % kVRing; r < b0 + 2; r++, vk = vk == kVRing - 1 ? 0 : vk + 1) {
+            // next iteration's model values (one row ahead): dt/rho and sponge of row r+1,
+            // stiffness of row r-1
             float buo_n[4], bnd_n[4], ip0_n[4], ip1_n[4];
-            ld_model(buo_n, a.buo, r + 1);
-            ld_model(bnd_n, a.bound, r + 1);
-            ld_model(ip0_n, a.ip[0], r - 1);
-            if (MODE == FWI_PSV) ld_model(ip1_n, a.ip[1], r - 1);
+            {
+                const long long m1 = (long long)(r + 1) * pitch + j0, m2 = m1 - 2ll * pitch;
+                const bool ok1 = tin && r + 1 < nx, ok2 = tin && r >= 1 && r - 1 < nx;
+#pragma unroll
+                for (int e = 0; e < 4; e++) buo_n[e] = bnd_n[e] = ip0_n[e] = ip1_n[e] = 0.f;
+                if (ok1) {
+                    ldg4(buo_n, a.buo + m1);
+                    ldg4(bnd_n, a.bound + m1);
+                }
+                if (ok2) {
+                    ldg4(ip0_n, a.ip[0] + m2);
+                    if (MODE == FWI_PSV) ldg4(ip1_n, a.ip[1] + m2);
+                }
+            }
+            // velocity-ring slots of rows r-3 .. r (row r-3+k in slot vs[k])
+            int vs[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int q = vk - 3 + k;
+                vs[k] = q < 0 ? q + kVRing : q;
+            }
+            auto vrow = [&](int slot, int c) -> float * { return smem + L.vring + (slot * NV + c) * RL + 4 + j0; };
             // the z window shifts: wz[0..2] <- rows r-2, r-1, r
 #pragma unroll
             for (int e = 0; e < 4; e++) {
@@ -454,7 +471,7 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
                             vn[c][e] = (!ZE || zin[e]) ? v : 0.f;  // padding columns stay zero
                             if (ZE && !zin[e]) ds[c][e] = 0.f;
                         }
-                        st4(vel_row(r, c) + j0, vn[c]);
+                        st4(vrow(vs[3], c), vn[c]);
                         if (own) {
                             st4(a.vel_out[c] + grow, vn[c]);
                             if (a.seg_ds[c]) st4(a.seg_ds[c] + grow, ds[c]);
@@ -491,7 +508,7 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
                 for (int c = 0; c < NV; c++) {
 #pragma unroll
                     for (int e = 0; e < 4; e++) vn[c][e] = 0.f;
-                    st4(vel_row(r, c) + j0, vn[c]);
+                    st4(vrow(vs[3], c), vn[c]);
                 }
             }
             // the next iteration reads row r+2: warp 0 waits for it before the barrier
@@ -515,13 +532,13 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
                     // rows s-1 .. s+2 of the new velocity, and row s's z neighbours:
                     // y[i] = column j0-1+i of row s
                     float v0[4], v1[4], v2[4], v3[4];
-                    ld4(v0, vel_row(s - 1, c) + j0);
-                    ld4(v1, vel_row(s, c) + j0);
-                    ld4(v2, vel_row(s + 1, c) + j0);
-                    ld4(v3, vel_row(s + 2, c) + j0);
-                    const float *vs = vel_row(s, c) + j0;
-                    const float l1 = vs[-1];
-                    const float2 r2 = *reinterpret_cast<const float2 *>(vs + 4);
+                    ld4(v0, vrow(vs[0], c));
+                    ld4(v1, vrow(vs[1], c));
+                    ld4(v2, vrow(vs[2], c));
+                    ld4(v3, vrow(vs[3], c));
+                    const float *vsr = vrow(vs[1], c);
+                    const float l1 = vsr[-1];
+                    const float2 r2 = *reinterpret_cast<const float2 *>(vsr + 4);
                     const float y[7] = {l1, v1[0], v1[1], v1[2], v1[3], r2.x, r2.y};
 #pragma unroll
                     for (int e = 0; e < 4; e++) {

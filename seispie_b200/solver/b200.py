@@ -256,20 +256,20 @@ class b200:
         """Misfit and exact gradient of this process's shots, accumulated in
         the reference's units (dt * dchi/dparam) into k_lam_f64 / k_mu_f64 /
         k_rho_f64; returns the misfit (sum of per-shot, per-component norms)."""
-        from ..adjoint import ExactAdjoint, fixed_bytes
+        from ..adjoint import ExactAdjoint, max_tail_bytes
         combine = self.config["combine_sources"] == "yes"
         misfit = 0.0
         nrec, nt = self.nrec, self.nt
         for chunk in self._chunks(shots, mode, True):
             n = len(chunk)
             with self._ctx():
-                # the last steps keep their per-step stores from the forward sweep in half of the HBM
-                # that the checkpoints and segment stores leave free (those steps are not recomputed;
-                # the gradient is the same); not when the configuration caps the memory of a batch
+                # the last steps keep their per-step stores from the forward sweep (those steps are not
+                # recomputed; the gradient is the same): the longest tail that fits 85 % of the free HBM
+                # with everything else the gradient holds; not when the configuration caps the memory
+                # of a batch
                 tail = 0.0
                 if self.batch_memory <= 0:
-                    spare = self._free_bytes() - fixed_bytes(nt, mode, n, self.model.grid, nrec)
-                    tail = 0.5 * max(0.0, spare)
+                    tail = max_tail_bytes(nt, mode, n, self.model.grid, 0.85 * self._free_bytes(), nrec)
                 ea = ExactAdjoint(self.model, nt, self.src_id, lambda s: -1 if combine else chunk[s], n,
                                   self._stf(mode), self.rec_id, tile=self.tile, tail_memory=tail)
                 # the observed traces are stacked into pinned host memory on worker threads while

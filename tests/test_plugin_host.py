@@ -134,3 +134,26 @@ def test_exact_adjoint_fixed_bytes():
     # a step stores 6 strain terms and 3 divergences, a batch holds 2 x (6 + 3) + 3 fields
     assert fixed_bytes(100, FWI_SPIN, 2, Grid(8, 8, 1.0, 1.0), 0, segment=10) == \
         (10 * 12 + 10 * 9 + 2 * 21) * 4 * 2 * 8 * 8
+
+
+def test_max_tail_bytes_is_the_longest_tail_that_fits():
+    """The stored tail is sized so that checkpoints (of the steps before it),
+    one segment of stores, the tail, both batches and the traces fit the
+    budget, and one more tail step would not."""
+    import math
+    from seispie_b200._lib import FWI_PSV
+    from seispie_b200.adjoint import default_segment, max_tail_bytes
+    from seispie_b200.engine import Grid
+    g = Grid(512, 510, 10.0, 10.0)  # pitch 512
+    nt, ns, nrec = 4000, 32, 256
+    field = 4 * ns * 512 * 512
+    k = default_segment(nt, FWI_PSV, ns, g)
+
+    def need(t):
+        return (math.ceil((nt - t) / k) * 5 + k * 5 + t * 5 + 20) * field + 3 * 4 * ns * nrec * nt * 2
+
+    for budget in (30e9, 100e9, 160e9):
+        t = max_tail_bytes(nt, FWI_PSV, ns, g, budget, nrec) // (5 * field)
+        assert 0 < t < nt and need(t) <= budget < need(t + 1)
+    assert max_tail_bytes(nt, FWI_PSV, ns, g, 1e9, nrec) == 0  # nothing fits: no tail
+    assert max_tail_bytes(100, FWI_PSV, 1, Grid(8, 8, 1.0, 1.0), 1e12, 0) == 100 * 5 * 4 * 8 * 8
