@@ -633,30 +633,10 @@ __global__ void displacement_traces_kernel(float *obs, long long ntr, int nt, in
 
 static int comp_slot_of(int mode, int q) { return mode == FWI_SH ? 1 : (q == 0 ? 0 : 2); }
 
-// Ring depth for a row length: the requested depth (3, 4, 6 or 8), or by
-// default the depth that lets the most CTAs share an SM (228 KB of shared
-// memory, 1 KB of it reserved per CTA), the deepest among those.  0 if it
-// does not fit.
-static int march_slots(int mode, int rl, int want, size_t *bytes) {
+// Shared-memory bytes of a ring depth for a row length.
+static size_t march_bytes(int mode, int rl, int n) {
     const int nf = mode == FWI_SH ? 3 : 5, nv = mode == FWI_SH ? 1 : 2, ninj = mode == FWI_SH ? 1 : 2;
-    const size_t sm = (size_t)228 * 1024, cap = (size_t)227 * 1024;
-    if (want) {
-        *bytes = march_layout(nf, nv, ninj, rl, want).bytes;
-        return *bytes <= cap ? want : 0;
-    }
-    int best = 0;
-    size_t best_ctas = 0;
-    for (int n : {3, 4, 6, 8}) {
-        const size_t b = march_layout(nf, nv, ninj, rl, n).bytes;
-        if (b > cap) continue;
-        const size_t ctas = sm / (b + 1024);
-        if (ctas >= best_ctas) {
-            best_ctas = ctas;
-            best = n;
-            *bytes = b;
-        }
-    }
-    return best;
+    return march_layout(nf, nv, ninj, rl, n).bytes;
 }
 
 bool march_supported(const fwi_batch *b) {
@@ -664,29 +644,72 @@ bool march_supported(const fwi_batch *b) {
 }
 
 template <int MODE, int N>
-static int launch_march_mode(const MarchArgs &a, int nthr, size_t bytes, cudaStream_t st) {
-    static size_t attr_bytes = 0;
-    static int sms = 0, occ = 0, occ_thr = 0;
-    static size_t occ_bytes = 0;
-    if (bytes > attr_bytes) {
-        cudaError_t e = cudaFuncSetAttribute(march_kernel<MODE, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)bytes);
-        if (e != cudaSuccess) return set_error(FWI_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
-        attr_bytes = bytes;
+static int march_occupancy(int nthr, size_t bytes, int *occ) {
+    cudaError_t e = cudaFuncSetAttribute(march_kernel<MODE, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, march_kernel<MODE, N>, nthr, bytes);
+    if (e != cudaSuccess) return set_error(FWI_ECUDA, "march_kernel occupancy: %s", cudaGetErrorString(e));
+    return 0;
+}
+
+template <int MODE>
+static int march_occupancy_n(int n, int nthr, size_t bytes, int *occ) {
+    switch (n) {
+        case 3: return march_occupancy<MODE, 3>(nthr, bytes, occ);
+        case 4: return march_occupancy<MODE, 4>(nthr, bytes, occ);
+        case 6: return march_occupancy<MODE, 6>(nthr, bytes, occ);
+        default: return march_occupancy<MODE, 8>(nthr, bytes, occ);
     }
+}
+
+// Ring depth and resident CTAs per SM for a launch shape: the requested
+// depth, or the one with the most resident CTAs (shared memory and
+// registers both counted), the deepest among those.  Cached per shape.
+template <int MODE>
+static int march_choose(int nthr, int rl, int want, int *n_out, size_t *bytes_out, int *occ_out) {
+    struct Entry {
+        int nthr, rl, want, n, occ;
+        size_t bytes;
+    };
+    static Entry cache[16];
+    static int ncache = 0;
+    for (int i = 0; i < ncache; i++)
+        if (cache[i].nthr == nthr && cache[i].rl == rl && cache[i].want == want) {
+            *n_out = cache[i].n;
+            *bytes_out = cache[i].bytes;
+            *occ_out = cache[i].occ;
+            return 0;
+        }
+    int best = 0, best_occ = 0;
+    size_t best_bytes = 0;
+    for (int n : {3, 4, 6, 8}) {
+        if (want && n != want) continue;
+        const size_t b = march_bytes(MODE, rl, n);
+        if (b > (size_t)227 * 1024) continue;
+        int occ = 0;
+        const int rc = march_occupancy_n<MODE>(n, nthr, b, &occ);
+        if (rc) return rc;
+        if (occ >= 1 && occ >= best_occ) {
+            best = n;
+            best_occ = occ;
+            best_bytes = b;
+        }
+    }
+    if (!best) return set_error(FWI_ERANGE, "row-marching step: rows of %d floats do not fit an SM", rl - 8);
+    if (ncache < 16) cache[ncache++] = Entry{nthr, rl, want, best, best_occ, best_bytes};
+    *n_out = best;
+    *bytes_out = best_bytes;
+    *occ_out = best_occ;
+    return 0;
+}
+
+template <int MODE, int N>
+static int launch_march_mode(const MarchArgs &a, int nthr, size_t bytes, int occ, cudaStream_t st) {
+    static int sms = 0;
     if (!sms) {
         int dev = 0;
         if (cudaGetDevice(&dev) != cudaSuccess ||
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
             sms = 148;
-    }
-    if (occ_thr != nthr || occ_bytes != bytes) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, march_kernel<MODE, N>, nthr, bytes) != cudaSuccess ||
-            occ < 1)
-            return set_error(FWI_ECUDA, "march_kernel: %d threads with %zu bytes of shared memory do not fit an SM",
-                             nthr, bytes);
-        occ_thr = nthr;
-        occ_bytes = bytes;
     }
     const long long grid = a.rows_total < (long long)sms * occ ? a.rows_total : (long long)sms * occ;
     march_kernel<MODE, N><<<(unsigned)grid, nthr, bytes, st>>>(a);
@@ -743,21 +766,23 @@ int launch_march(const fwi_batch *b, int it, cudaStream_t st) {
     const int nthr = ((b->pitch / 4 + 31) / 32) * 32;
     a.rl = 4 * nthr + 8;
     size_t bytes = 0;
-    const int n = march_slots(mode, a.rl, b->ring, &bytes);
-    if (!n) return set_error(FWI_ERANGE, "row-marching step: rows of %d columns do not fit shared memory", b->pitch);
+    int n = 0, occ = 0;
+    int rc = mode == FWI_SH ? march_choose<FWI_SH>(nthr, a.rl, b->ring, &n, &bytes, &occ)
+                            : march_choose<FWI_PSV>(nthr, a.rl, b->ring, &n, &bytes, &occ);
+    if (rc) return rc;
     if (mode == FWI_SH) {
         switch (n) {
-            case 3: return launch_march_mode<FWI_SH, 3>(a, nthr, bytes, st);
-            case 4: return launch_march_mode<FWI_SH, 4>(a, nthr, bytes, st);
-            case 6: return launch_march_mode<FWI_SH, 6>(a, nthr, bytes, st);
-            default: return launch_march_mode<FWI_SH, 8>(a, nthr, bytes, st);
+            case 3: return launch_march_mode<FWI_SH, 3>(a, nthr, bytes, occ, st);
+            case 4: return launch_march_mode<FWI_SH, 4>(a, nthr, bytes, occ, st);
+            case 6: return launch_march_mode<FWI_SH, 6>(a, nthr, bytes, occ, st);
+            default: return launch_march_mode<FWI_SH, 8>(a, nthr, bytes, occ, st);
         }
     }
     switch (n) {
-        case 3: return launch_march_mode<FWI_PSV, 3>(a, nthr, bytes, st);
-        case 4: return launch_march_mode<FWI_PSV, 4>(a, nthr, bytes, st);
-        case 6: return launch_march_mode<FWI_PSV, 6>(a, nthr, bytes, st);
-        default: return launch_march_mode<FWI_PSV, 8>(a, nthr, bytes, st);
+        case 3: return launch_march_mode<FWI_PSV, 3>(a, nthr, bytes, occ, st);
+        case 4: return launch_march_mode<FWI_PSV, 4>(a, nthr, bytes, occ, st);
+        case 6: return launch_march_mode<FWI_PSV, 6>(a, nthr, bytes, occ, st);
+        default: return launch_march_mode<FWI_PSV, 8>(a, nthr, bytes, occ, st);
     }
 }
 
