@@ -7,22 +7,34 @@ model, homogeneous start) / rho 2600, 32 Ricker sources (f0 = 8 Hz) evenly
 spaced at z = 10 cells, 256 receivers at z = 12 cells, dt = 1e-3 s,
 nt = 4000, 20-cell sponge on the left, right and bottom, adjoint interval 10,
 smoothing sigma 4.  Observed data come from the checkerboard model (computed
-once, untimed).  One step = one gradient of all 32 shots: batched forward with
-checkpoints, misfit and trace gradients, exact discrete adjoint (checkpointed
-recomputation + transposed steps with the lambda / mu / rho terms), Gaussian
-smoothing (``--gradient reference``: forward with snapshots and the
+once, untimed).  One step = one gradient of all shots: batched forward with
+checkpoints (row-marching step kernel, no displacement field), misfit and
+trace gradients, exact discrete adjoint (checkpointed recomputation +
+transposed steps with the lambda / mu / rho terms), Gaussian smoothing
+(``--gradient reference``: forward with snapshots and the
 snapshot-correlation adjoint instead).  Cell-updates per step =
-32 * 512 * 512 * 4000 * 2 (forward and adjoint counted separately; recomputed
-forward steps are not counted).
+shots * 512 * 512 * 4000 * 2 (forward and adjoint counted separately;
+recomputed forward steps are not counted).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--shard]
+
+On N GPUs (torchrun, one rank per GPU) every rank owns a contiguous block of
+the shots and the ranks sum the FP64 mu kernel and the misfit with one
+all-reduce before the smoothing, as the reference sums before it smooths
+(solver.py:375-396).  By default each rank has 32 shots (the survey grows
+with N: weak scaling); ``--shard`` splits the 32 shots over the ranks
+(strong scaling).
 
 Prints one JSON line (rank 0).  ``value`` is measured with every input in HBM;
 ``e2e`` through the plugin API (seispie_b200.solver.b200.compute_gradient)
 with the observed traces in host memory, their upload and the gradient's
-download inside the timed region.  ``--impl reference`` times the CPU
-restatement of the reference's arithmetic (oracle/, float32, all host threads)
-on a bounded sample of the same workload.
+download inside the timed region.  ``roofline`` is the row-marching step
+kernel's (CUDA events around its launches inside the timed region);
+``gradient_roofline`` the whole gradient's useful cell-update rate in the
+same bytes.  ``--impl reference`` times the CPU restatement of the
+reference's arithmetic (oracle/, float32, all host threads) on a bounded
+sample of the same workload, and reports beside it the unmodified reference
+timed under Numba's CUDA simulator (oracle/reference_cudasim.json).
 """
 from __future__ import annotations
 
@@ -66,6 +78,8 @@ def parse():
     ap.add_argument("--profile-case", action="store_true",
                     help="only run a few forward steps (for ncu captures of the step kernel)")
     ap.add_argument("--autotune", action="store_true", help="time every tile variant and report the best")
+    ap.add_argument("--shard", action="store_true",
+                    help="split the --shots shots over the ranks (strong scaling) instead of --shots per rank")
     ap.add_argument("--gradient", default="exact", choices=["exact", "reference"],
                     help="exact: discrete adjoint with checkpointing (the solver's P-SV gradient); "
                          "reference: snapshot-correlation adjoint of the reference's algorithm")
@@ -74,7 +88,14 @@ def parse():
 
 # ------------------------------------------------------------------ workload
 
-def workload(a):
+def total_shots(a, world):
+    """Shots of the whole job: --shots per rank, or --shots split over the
+    ranks with --shard."""
+    return a.shots if a.shard else a.shots * world
+
+
+def workload(a, nshots=None):
+    nshots = a.shots if nshots is None else nshots
     nx, nz, h = a.nx, a.nz, 10.0
     i, j = np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij")
     sign = np.where(((i // 32) + (j // 32)) % 2 == 0, 1.0, -1.0)
@@ -84,18 +105,21 @@ def workload(a):
     rho = np.full(n, 2600.0, np.float32)
     vs_init = np.full(n, 1732.0, np.float32)
     f0 = 8.0
-    src = np.array([[(s + 0.5) * nx / a.shots * h, 10 * h, 0, f0, 1.2 / f0, 0.0, 1e10] for s in range(a.shots)])
+    src = np.array([[(s + 0.5) * nx / nshots * h, 10 * h, 0, f0, 1.2 / f0, 0.0, 1e10] for s in range(nshots)])
     rec = np.array([[(r + 0.5) * nx / a.nrec * h, 12 * h] for r in range(a.nrec)])
     return dict(nx=nx, nz=nz, h=h, dt=1e-3, vp=vp, rho=rho, vs_true=vs_true, vs_init=vs_init, src=src, rec=rec,
                 absorb=(20, 0.015, 1, 1, 1, 0))
 
 
-def config_of(a, w, extra=None):
+def config_of(a, w, extra=None, world=1):
+    ns = total_shots(a, world)
     c = {"workload": "psv_gradient_%dx%d_shots%d_rec%d_nt%d" % (a.nx, a.nz, a.shots, a.nrec, a.nt),
-         "grid": [a.nx, a.nz], "shots": a.shots, "receivers": a.nrec, "nt": a.nt, "adjoint_interval": a.sae,
-         "smooth_sigma": a.sigma, "cells_per_step": 2 * a.shots * a.nx * a.nz * a.nt,
-         "l2": "inputs larger than L2 (each wavefield field of the 32 shots is 32 MiB, the state 7 fields, the checkpoints 23 GiB: far above the 126 MB L2); no flush",
-         "parallelism": "shots", "gradient": a.gradient}
+         "grid": [a.nx, a.nz], "shots": ns, "shots_per_rank": ns // world, "receivers": a.nrec, "nt": a.nt,
+         "adjoint_interval": a.sae, "smooth_sigma": a.sigma, "cells_per_step": 2 * ns * a.nx * a.nz * a.nt,
+         "l2": "inputs larger than L2 (each wavefield field of 32 shots is 32 MiB, the state 5 fields, the "
+               "checkpoints and stored steps ~150 GB: far above the 126 MB L2); no flush",
+         "parallelism": "shots (contiguous blocks per rank, one FP64 all-reduce per gradient)"
+                        if world > 1 else "shots", "gradient": a.gradient}
     if extra:
         c.update(extra)
     return c
@@ -161,8 +185,11 @@ class ClockSampler:
 
 def cpu_sample(a, w, seconds):
     """Time the oracle's float32 restatement of the reference (forward and
-    adjoint of one shot, all host threads) for about ``seconds``; returns
-    (cell-updates/s, sample description, threads)."""
+    adjoint of one shot, all host threads) for about ``seconds``.  The
+    adjoint timed is the reference's snapshot-correlation adjoint
+    (solver.py:290-321, extended to P-SV), which does less work than the
+    exact adjoint with recomputation the GPU runs.  Returns (cell-updates/s,
+    sample dict, threads)."""
     from oracle.oracle import Oracle, point_ids, source_time_functions
     o = Oracle("f32")
     nx, nz, h, dt = w["nx"], w["nz"], w["h"], w["dt"]
@@ -188,27 +215,54 @@ def cpu_sample(a, w, seconds):
     o.adjoint_psv(nx, nz, h, h, dt, nt, p, rid, ad, ad, a.sae, sn, k[0], k[1], k[2])
     el = time.perf_counter() - t
     threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    sample = "1 shot of %dx%d, nt=%d forward+adjoint (oracle float32 restatement of the reference)" % (nx, nz, nt)
-    return 2 * nx * nz * nt / el / 1e9, sample, threads
+    cells = 2 * nx * nz * nt
+    sample = {"what": "1 shot of %dx%d, nt=%d: forward + snapshot-correlation adjoint of the float32 oracle "
+                      "(the reference's arithmetic)" % (nx, nz, nt),
+              "shots": 1, "nt": nt, "cell_updates": cells, "seconds": el}
+    return cells / el / 1e9, sample, threads
+
+
+def reference_cudasim():
+    """The unmodified reference timed under Numba's CUDA simulator by
+    oracle/time_reference.py (measured where that script ran, recorded in
+    oracle/reference_cudasim.json), or None."""
+    try:
+        rec = json.load(open(os.path.join(ROOT, "oracle", "reference_cudasim.json")))
+    except Exception:
+        return None
+    c = rec["cases"]
+    return {"value": c["psv_forward"]["cell_updates_per_s"] / 1e9, "unit": UNIT, "cores": rec["cores_used"],
+            "kind": "reference", "nproc": rec["nproc"],
+            "sample": rec["what"] + " (P-SV forward; the reference's P-SV adjoint cannot run; SH gradient "
+                                    "%.3g cell-updates/s)" % c["sh_gradient"]["cell_updates_per_s"],
+            "measured": "build container (numba %s), not the GPU host: the reference's Python source does not "
+                        "travel to the GPU box" % rec["numba"]}
 
 
 def run_reference(a):
+    """Reference arm: the CPU restatement of the reference's arithmetic on a
+    bounded sample of the workload per step; ms_per_step is the sample's own
+    time."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     w = workload(a)
-    vals = []
+    vals, secs = [], []
     sample = threads = None
     for s in range(a.warmup + a.steps):
         v, sample, threads = cpu_sample(a, w, a.cpu_seconds / max(1, a.steps))
         if s >= a.warmup:
             vals.append(v)
+            secs.append(sample["seconds"])
     v = statistics.median(vals)
+    cfg = config_of(a, w)
+    cfg["cells_per_step"] = sample["cell_updates"]  # each step is one bounded sample
     line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": a.gpus, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": 2 * a.shots * a.nx * a.nz * a.nt / (v * 1e9) * 1e3,
+            "warmup": a.warmup, "ms_per_step": statistics.median(secs) * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": config_of(a, w),
+            "data": "synthetic", "config": cfg,
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "reference_cudasim": reference_cudasim(),
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -233,9 +287,12 @@ def main():
 
     from seispie_b200 import _lib, engine
     from seispie_b200.engine import Grid, ShotBatch, adjoint_injection_lists, build_model, injection_lists
+    from seispie_b200.parallel import shard
 
     lib = _lib.load()
-    w = workload(a)
+    ntot = total_shots(a, world)
+    mine = list(shard(ntot, rank, world))  # this rank's contiguous block of shots
+    w = workload(a, ntot)
     nx, nz, h, dt, nt = w["nx"], w["nz"], w["h"], w["dt"], a.nt
     sid = engine.point_ids(w["src"], np.float32(h), np.float32(h), nz)
     rid = engine.point_ids(w["rec"], np.float32(h), np.float32(h), nz)
@@ -243,8 +300,8 @@ def main():
     m_true = build_model("psv", grid, dt, dict(vp=w["vp"], vs=w["vs_true"], rho=w["rho"]), w["absorb"], dev)
     m_init = build_model("psv", grid, dt, dict(vp=w["vp"], vs=w["vs_init"], rho=w["rho"]), w["absorb"], dev)
     stf, _ = engine.ricker_stf(w["src"], nt, dt, dev)
-    nshots = a.shots
-    inj = injection_lists(nshots, sid, lambda s: s)
+    nshots = len(mine)
+    inj = injection_lists(nshots, sid, lambda s: mine[s])
 
     if a.profile_case:
         b = ShotBatch(m_init, nshots, nt, rid, tile=a.tile)
@@ -264,6 +321,16 @@ def main():
 
     stream = torch.cuda.current_stream()
     ev = {}
+
+    def reduce_and_smooth(mis, k_mu):
+        """Sum the ranks' FP64 mu kernels and misfits, then smooth (the
+        reference's order, solver.py:375-396)."""
+        m = torch.stack([x.sum() for x in mis]).sum()
+        if world > 1:
+            dist.all_reduce(k_mu)
+            dist.all_reduce(m)
+        return m, engine.smooth(k_mu, m_init.grid, a.sigma)
+
     if a.gradient == "exact":
         # exact discrete adjoint with checkpointed recomputation (the P-SV gradient of the solver)
         from seispie_b200._lib import FWI_PSV
@@ -272,7 +339,7 @@ def main():
         # 90 % of the free HBM with the checkpoints, segment stores, wavefields and traces
         free, _ = torch.cuda.mem_get_info(dev)
         tail = max_tail_bytes(nt, FWI_PSV, nshots, m_init.grid, 0.9 * free, a.nrec)
-        ea = ExactAdjoint(m_init, nt, sid, lambda s: s, nshots, stf, rid, tile=a.tile, tail_memory=tail)
+        ea = ExactAdjoint(m_init, nt, sid, lambda s: mine[s], nshots, stf, rid, tile=a.tile, tail_memory=tail)
         checkpointing = {"segment": ea.K, "checkpoints": ea.nseg, "stored_tail_steps": ea.tail}
         grads = [torch.empty((nshots, a.nrec, nt), dtype=torch.float32, device=dev) if c != 1 else None
                  for c in range(3)]
@@ -282,6 +349,7 @@ def main():
 
         def gradient(record=False):
             e0, e1, e2, e3 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
+            ea.step_events = ev.setdefault("steps", []) if record else None
             e0.record(stream)
             tr = ea.forward()
             e1.record(stream)
@@ -290,13 +358,11 @@ def main():
             e2.record(stream)
             k_lam, k_mu, k_buo = ea.backward(grads)
             e3.record(stream)
-            g = engine.smooth(k_mu, m_init.grid, a.sigma)
-            if world > 1:
-                dist.all_reduce(k_mu)
+            m, g = reduce_and_smooth(mis, k_mu)
             if record:
                 ev.setdefault("fwd", []).append((e0, e1))
                 ev.setdefault("adj", []).append((e2, e3))
-            return mis, g
+            return m, g
     else:
         nsa = nt // a.sae
         b = ShotBatch(m_init, nshots, nt, rid, sae=a.sae, nsa=nsa, snapshots=True, tile=a.tile)
@@ -321,13 +387,11 @@ def main():
             e2.record(stream)
             b.run(adj, True, 0, nt)
             e3.record(stream)
-            g = engine.smooth(k_mu, m_init.grid, a.sigma)
-            if world > 1:
-                dist.all_reduce(k_mu)
+            m, g = reduce_and_smooth(mis, k_mu)
             if record:
                 ev.setdefault("fwd", []).append((e0, e1))
                 ev.setdefault("adj", []).append((e2, e3))
-            return mis, g
+            return m, g
 
     def tune():
         from seispie_b200.autotune import autotune
@@ -360,32 +424,50 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
         dist.barrier()
-    cells_rank = 2 * nshots * nx * nz * nt
-    value = cells_rank * world / (ms * 1e-3) / 1e9
+    cells = 2 * ntot * nx * nz * nt  # useful cell-updates of the whole job per step
+    value = cells / (ms * 1e-3) / 1e9
 
-    # roofline of the dominant kernel: the fused P-SV step (forward launches)
-    fwd_ms = statistics.median(e0.elapsed_time(e1) for e0, e1 in ev["fwd"])
-    adj_ms = statistics.median(e0.elapsed_time(e1) for e0, e1 in ev["adj"])
-    per_launch_s = fwd_ms * 1e-3 / nt
-    bytes_per_launch = nshots * nx * nz * (72 + 8.0 / a.sae)
-    achieved = bytes_per_launch / per_launch_s / 1e9
     peak, peak_src = 6650.0, "fallback"
     try:
         pk = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         peak, peak_src = float(pk["hbm_gbs"]), "measured"
     except Exception:
         pass
+    fwd_ms = statistics.median(e0.elapsed_time(e1) for e0, e1 in ev["fwd"])
+    adj_ms = statistics.median(e0.elapsed_time(e1) for e0, e1 in ev["adj"])
+    if a.gradient == "exact":
+        # the dominant kernel: the row-marching step, timed launch by launch (CUDA events around the plain
+        # forward segments of every timed gradient; each segment adds one short trace-conversion launch)
+        steps = ev.get("steps", [])
+        n_launch = sum(n for _, _, n in steps)
+        per_launch_s = sum(e0.elapsed_time(e1) for e0, e1, _ in steps) * 1e-3 / max(1, n_launch)
+        # algorithmic bytes: stress (3) and velocity (2) read and written, lam, mu, dt/rho, sponge read
+        bytes_per_launch = nshots * nx * nz * (40 + 16)
+        kernel = "march_kernel<P-SV> (row-marching step, displacement-free; plain forward launches)"
+        traffic_file = "march_kernel_psv_traffic.json"
+    else:
+        per_launch_s = fwd_ms * 1e-3 / nt
+        bytes_per_launch = nshots * nx * nz * (72 + 8.0 / a.sae)
+        kernel = "step_kernel<P-SV> (tiled, with displacement and snapshots; forward sweep / nt)"
+        traffic_file = "step_kernel_psv_traffic.json"
+    achieved = bytes_per_launch / per_launch_s / 1e9
     traffic = None
     try:
-        prof = json.load(open(os.path.join(ROOT, "profiles", "step_kernel_psv_traffic.json")))
-        traffic = prof["dram_bytes_per_launch_full_workload"]
+        prof = json.load(open(os.path.join(ROOT, "profiles", traffic_file)))
+        traffic = prof["dram_bytes_per_launch_full_workload"] * nshots / prof.get("shots", 32)
     except Exception:
         pass
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": traffic, "peak_source": peak_src, "kernel": "step_kernel<P-SV> (forward launches)",
+            "traffic": traffic, "peak_source": peak_src, "kernel": kernel,
             "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_us": per_launch_s * 1e6,
-            "adjoint_step_us": adj_ms * 1e3 / nt}
-    misfit_total = float(sum(m.sum().item() for m in mis))
+            "launches_timed": n_launch if a.gradient == "exact" else nt,
+            "forward_sweep_us_per_step": fwd_ms * 1e3 / nt, "backward_us_per_step": adj_ms * 1e3 / nt}
+    # the whole gradient: useful cell-updates per second per GPU times the P-SV algorithmic bytes of a
+    # cell-update (72 B), against the same peak
+    grad_roof = {"bytes_per_cell_update": 72, "achieved": value / world * 72, "peak": peak, "unit": "GB/s",
+                 "frac": value / world * 72 / peak,
+                 "basis": "useful forward+adjoint cell-updates (recomputed steps not counted) x 72 B"}
+    misfit_total = float(mis.item())
     del b, fwd, adj
     ea = grads = None  # noqa: F841  (release the checkpoint buffers before the e2e run)
     torch.cuda.empty_cache()
@@ -393,7 +475,7 @@ def main():
     # ----------------------------------------------------------------- e2e
     e2e = None
     if not a.no_e2e:
-        e2e = run_e2e(a, w, dev, world, rank, data)
+        e2e = run_e2e(a, w, dev, world, rank, data, ntot)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -404,13 +486,15 @@ def main():
         extra = {"tile": _lib.tile_label(b_tile(a, tuned)), "misfit": misfit_total}
         if a.gradient == "exact":
             extra["checkpointing"] = checkpointing
+            extra["tile"] = "row-marching (displacement-free)"
         if tuned:
             extra["autotune_ms_per_fwd_step"] = tuned[2]
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
-                "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config_of(a, w, extra),
-                "clocks": clk.summary(), "gpu_launches": launches, "roofline": roof, "e2e": e2e,
-                "cpu_baseline": cpu, "impl": "b200"}
+                "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
+                "scaling": "strong" if a.shard else "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": config_of(a, w, extra, world), "clocks": clk.summary(),
+                "gpu_launches": launches, "roofline": roof, "gradient_roofline": grad_roof, "e2e": e2e,
+                "cpu_baseline": cpu, "reference_cudasim": reference_cudasim() if cpu else None, "impl": "b200"}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -421,8 +505,9 @@ def b_tile(a, tuned):
     return tuned[0] if tuned else a.tile
 
 
-def run_e2e(a, w, dev, world, rank, data):
-    """compute_gradient() of the b200 plugin with host-resident traces."""
+def run_e2e(a, w, dev, world, rank, data, ntot):
+    """compute_gradient() of the b200 plugin with host-resident traces (on N
+    ranks through the plugin's own shot sharding and kernel sum)."""
     import torch
     from seispie_b200.solver import b200
 
@@ -440,23 +525,30 @@ def run_e2e(a, w, dev, world, rank, data):
                     tile=str(a.tile))
     s.path = dict(model_init=td + "/init", model_true=td + "/init", sources=td + "/src.dat",
                   stations=td + "/rec.dat", output=td + "/out")
-    s.mpi = None
+    if world > 1:
+        from seispie_b200.parallel import TorchMPI
+        s.mpi = TorchMPI()  # the process group bench.py opened
+    else:
+        s.mpi = None
     with contextlib.redirect_stdout(io.StringIO()):
         s.setup(None)
         s.import_model(0)
         s.import_sources()
         s.import_stations()
-    dx = data[0].view(a.shots, a.nrec * a.nt).cpu().numpy()
-    dz = data[2].view(a.shots, a.nrec * a.nt).cpu().numpy()
-    s.syn_x = [np.ascontiguousarray(dx[i]) for i in range(a.shots)]
-    s.syn_z = [np.ascontiguousarray(dz[i]) for i in range(a.shots)]
+    nloc = len(s._shots())  # this rank's shots, in the order of `data`
+    dx = data[0].view(nloc, a.nrec * a.nt).cpu().numpy()
+    dz = data[2].view(nloc, a.nrec * a.nt).cpu().numpy()
+    s.syn_x = [np.ascontiguousarray(dx[i]) for i in range(nloc)]
+    s.syn_z = [np.ascontiguousarray(dz[i]) for i in range(nloc)]
     s.syn_y = []
-    h2d = sum(x.nbytes for x in s.syn_x + s.syn_z)
+    h2d = sum(x.nbytes for x in s.syn_x + s.syn_z) * world
     d2h = 2 * nx * nz * 4  # gradient and model returned as float32
     with contextlib.redirect_stdout(io.StringIO()):
         for _ in range(max(1, a.warmup)):
             s.compute_gradient()
         torch.cuda.synchronize()
+        if world > 1:
+            s.mpi.sync()
         t = time.perf_counter()
         for _ in range(a.steps):
             s.compute_gradient()
@@ -467,7 +559,7 @@ def run_e2e(a, w, dev, world, rank, data):
         tt = torch.tensor([el], device=dev)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         el = float(tt.item())
-    cells = 2 * a.shots * nx * nz * a.nt * world
+    cells = 2 * ntot * nx * nz * a.nt
     return {"value": cells / el / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
             "ms_per_step": el * 1e3, "api": "seispie_b200.solver.b200.compute_gradient"}
 

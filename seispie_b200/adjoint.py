@@ -149,6 +149,9 @@ class ExactAdjoint:
         self.t0 = self.nt - self.tail  # steps [t0, nt) keep their stores from the forward sweep
         self.nseg = math.ceil(self.t0 / self.K)
         self.fwd = ShotBatch(model, self.nshots, self.nt, self.rec_id, tile=tile)
+        # a list to collect (start, end, steps) CUDA events of the checkpointed forward segments
+        # (plain steps, no stores), or None
+        self.step_events = None
         inj = injection_lists(self.nshots, src_id, isrc_of_shot)
         self.fdesc = self.fwd.desc(inj=inj, stf=stf)
         # recomputed steps record no traces (the forward sweep has them)
@@ -188,7 +191,13 @@ class ExactAdjoint:
             for v in b.vel[b.cur]:
                 engine.energy_accumulate(v, self.illum)
             n = min(self.K, self.t0 - s * self.K)
+            if self.step_events is not None:  # CUDA events around the plain forward steps
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(torch.cuda.current_stream() if b.stream is None else b.stream)
             b.run(self.fdesc, False, s * self.K, n)
+            if self.step_events is not None:
+                e1.record(torch.cuda.current_stream() if b.stream is None else b.stream)
+                self.step_events.append((e0, e1, n))
         if self.tail:
             # the illumination is sampled at the multiples of K whatever the tail, so that it does not
             # depend on how much memory the tail got

@@ -80,3 +80,57 @@ def test_torch_mpi_shim_two_ranks_gloo():
     for _, _, k, m in res:
         assert m == total
         assert k == [float(i * total) for i in range(5)]
+
+
+class _NoStream:
+    def synchronize(self):
+        pass
+
+
+def _plugin_rank_main(rank, size, port, nsrc, q):
+    """One rank of the plugin's shot sharding: the solver's own _shots,
+    _mpi_sum_kernels and _mpi_sum_misfit on CPU kernels."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(size))
+    import torch
+    from seispie_b200.parallel import TorchMPI
+    from seispie_b200.solver.b200 import b200
+    mpi = TorchMPI("gloo")
+    try:
+        s = b200()
+        s.nsrc, s.mpi, s.stream = nsrc, mpi, _NoStream()
+        shape = (3, 4)
+        for name in ("k_lam_f64", "k_mu_f64", "k_rho_f64", "illum_f64", "k_nu_f64", "k_mnc_f64", "k_j_f64"):
+            setattr(s, name, torch.zeros(shape, dtype=torch.float64))
+        misfit = 0.0
+        for shot in s._shots():  # each shot adds a distinct power of two: a double count would show
+            for f, k in enumerate(s._summed_fields()):
+                k += float(2 ** shot) * (f + 1)
+            misfit += float(2 ** shot)
+        misfit = s._mpi_sum_misfit(misfit)
+        s._mpi_sum_kernels()
+        q.put((rank, list(s._shots()), [float(k[0, 0]) for k in s._summed_fields()], misfit))
+    finally:
+        mpi.close()
+
+
+def test_plugin_shot_sharding_and_kernel_sum_two_ranks_gloo():
+    """Two gloo ranks run the plugin's shot sharding: contiguous shards that
+    cover every shot once, and kernels and misfit summed across ranks so
+    that every shot counts exactly once (the reference's file exchange,
+    solver.py:380-391, added the local kernel twice)."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 30500 + os.getpid() % 1000
+    nsrc = 7
+    procs = [ctx.Process(target=_plugin_rank_main, args=(r, 2, port, nsrc, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert res[0][1] + res[1][1] == list(range(nsrc))  # contiguous, disjoint, complete
+    total = float(2 ** nsrc - 1)
+    for _, _, ks, m in res:
+        assert m == total
+        assert ks == [total * (f + 1) for f in range(7)]
