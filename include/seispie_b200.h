@@ -143,6 +143,19 @@ long long fwi_launch_count(void);
  * counterpart in the reference. */
 int fwi_device_status(int *status, int clear);
 
+/* Poll limit of every bounded wait in the library's kernels (0 restores the
+ * default of 2^22 polls, seconds on a B200).  A wait that runs out ends its
+ * kernel, which sets bit 0 (step kernels) or bit 1 (U-Net kernels) of
+ * fwi_device_status.  Synchronous; process-wide for the current device.  No
+ * counterpart in the reference. */
+int fwi_set_wait_limit(int polls);
+
+/* Launch a one-thread kernel whose bounded wait runs out (an mbarrier nothing
+ * completes; no copy in flight): it sets bit 0 of fwi_device_status and
+ * returns.  Tests the failure path without faulting or hanging the GPU.  No
+ * counterpart in the reference. */
+int fwi_wait_selftest(void *stream);
+
 /* Copy the last error message of the calling thread into buf (always NUL
  * terminated); returns the status code of that error (0 if none). */
 int fwi_last_error(char *buf, size_t len);

@@ -67,6 +67,8 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
         "fwi_binary_version": ([], ctypes.c_int),
         "fwi_last_error": ([ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
         "fwi_device_status": ([ctypes.POINTER(ctypes.c_int), ctypes.c_int], ctypes.c_int),
+        "fwi_set_wait_limit": ([ctypes.c_int], ctypes.c_int),
+        "fwi_wait_selftest": ([_vp], ctypes.c_int),
         "fwi_unet_conv_path": ([ctypes.c_int], ctypes.c_int),
         "fwi_tile_shape": ([ctypes.c_int, _ip, _ip], ctypes.c_int),
         "fwi_tile_kind": ([ctypes.c_int], ctypes.c_int),

@@ -312,6 +312,7 @@ class Seismograms(torch.autograd.Function):
         for i, c in enumerate(ctx.comps):
             gt[c] = grad[i]
         k_lam, k_mu, k_buo = ctx.ea.backward(gt)
+        engine.check_device(None, "Seismograms.backward")
         nz = g.nz
         dlam = k_lam[:, :nz].reshape(g.nx, nz)
         dmu = k_mu[:, :nz].reshape(g.nx, nz)

@@ -40,6 +40,7 @@ int launch_march(const fwi_batch *b, int it, cudaStream_t st);
 bool march_supported(const fwi_batch *b);
 int launch_displacement_traces(float *obs, long long ntr, int nt, int it0, int n, double dt, cudaStream_t st);
 int kernel_binary_version(int *v);
+int launch_wait_selftest(cudaStream_t st);
 long long multi_workspace_bytes(int n);
 int multi_prepare(fwi_batch *const *bs, int n, void *ws, int (*check)(const fwi_batch *, int, int, int));
 int multi_run(fwi_batch *const *bs, int n, void *ws, int it0, int nsteps, cudaStream_t st);
@@ -161,6 +162,18 @@ int fwi_device_status(int *status, int clear) {
     *status = (a || m ? 1 : 0) | (b ? 2 : 0);
     return 0;
 }
+
+int fwi_set_wait_limit(int polls) {
+    REQUIRE(polls >= 0, "fwi_set_wait_limit: polls must be >= 0 (0 restores the default)");
+    const int p = polls ? polls : kDefaultWaitPolls;
+    cudaError_t e = step_set_wait_limit(p);
+    if (e == cudaSuccess) e = march_set_wait_limit(p);
+    if (e == cudaSuccess) e = unet_set_wait_limit(p);
+    if (e != cudaSuccess) return set_error(FWI_ECUDA, "fwi_set_wait_limit: %s", cudaGetErrorString(e));
+    return 0;
+}
+
+int fwi_wait_selftest(void *stream) { return launch_wait_selftest((cudaStream_t)stream); }
 
 int fwi_last_error(char *buf, size_t len) {
     if (buf && len) {

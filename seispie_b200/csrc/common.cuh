@@ -65,12 +65,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait: gives up after ~2^22 polls (each poll may suspend the warp
-// for a while), so a lost transaction ends the kernel instead of hanging it.
+// Poll limit of the bounded waits (each translation unit has its own copy,
+// set through set_wait_limit_here; fwi_set_wait_limit sets them all).
+constexpr int kDefaultWaitPolls = 1 << 22;
+static __device__ int g_wait_polls = kDefaultWaitPolls;
+
+// Bounded wait: gives up after g_wait_polls polls (each poll may suspend the
+// warp for a while), so a lost transaction ends the kernel instead of hanging
+// it.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-    for (int i = 0; i < (1 << 22); i++)
+    const int polls = g_wait_polls;
+    for (int i = 0; i < polls; i++)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
+}
+
+// Host: set this translation unit's poll limit (synchronous).
+static inline cudaError_t set_wait_limit_here(int polls) {
+    return cudaMemcpyToSymbol(g_wait_polls, &polls, sizeof(int));
 }
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int c0, int c1, int c2,
                                             uint64_t *bar) {
@@ -128,5 +140,9 @@ int check_launch(const char *what);
 int step_device_status(int clear, int *status);
 int march_device_status(int clear, int *status);
 int unet_device_status(int clear, int *status);
+// Poll limits of the bounded waits of step.cu, march.cu and unet.cu.
+cudaError_t step_set_wait_limit(int polls);
+cudaError_t march_set_wait_limit(int polls);
+cudaError_t unet_set_wait_limit(int polls);
 
 }  // namespace fwi

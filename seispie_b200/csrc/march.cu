@@ -786,6 +786,24 @@ int launch_march(const fwi_batch *b, int it, cudaStream_t st) {
     }
 }
 
+// A bounded wait on an mbarrier that nothing ever completes: the wait runs
+// out after the current poll limit, the kernel records it in the status word
+// like a step kernel whose copies were lost, and returns.  No copy is in
+// flight, so giving up is harmless; used to test the failure path.
+__global__ void wait_selftest_kernel() {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        if (!mbar_wait(&bar, 0)) atomicExch(&g_march_status, 1);
+    }
+}
+
+int launch_wait_selftest(cudaStream_t st) {
+    wait_selftest_kernel<<<1, 32, 0, st>>>();
+    return check_launch("wait_selftest_kernel");
+}
+
 // Binary version (major*10 + minor) of the device code the library loaded.
 int kernel_binary_version(int *v) {
     cudaFuncAttributes fa;
@@ -803,3 +821,5 @@ int launch_displacement_traces(float *obs, long long ntr, int nt, int it0, int n
 }
 
 }  // namespace fwi
+
+cudaError_t fwi::march_set_wait_limit(int polls) { return fwi::set_wait_limit_here(polls); }

@@ -1681,3 +1681,5 @@ int launch_adjoint_step(const fwi_batch *b, int it, cudaStream_t st) {
 }
 
 }  // namespace fwi
+
+cudaError_t fwi::step_set_wait_limit(int polls) { return fwi::set_wait_limit_here(polls); }

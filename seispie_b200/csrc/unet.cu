@@ -915,3 +915,5 @@ int fwi_unet_mse(const float *out, const float *tgt, float *gout, double *loss, 
 }
 
 }  // extern "C"
+
+cudaError_t fwi::unet_set_wait_limit(int polls) { return fwi::set_wait_limit_here(polls); }

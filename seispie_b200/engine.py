@@ -351,6 +351,21 @@ def ricker_stf(src: np.ndarray, nt: int, dt: float, device, stream=None):
     return out, par
 
 
+def check_device(stream=None, what: str = "") -> None:
+    """Wait for ``stream`` (torch's current stream when None), then read and
+    clear the library's device status: if a bounded wait in one of its
+    kernels gave up (a copy that never landed), the results written since
+    the last check are invalid, and this raises FwiError."""
+    s = torch.cuda.current_stream() if stream is None else stream
+    s.synchronize()
+    v = ctypes.c_int()
+    check(_lib.load().fwi_device_status(ctypes.byref(v), 1), "fwi_device_status")
+    if v.value:
+        kinds = [k for bit, k in ((1, "step"), (2, "U-Net")) if v.value & bit]
+        raise _lib.FwiError("%s: a bounded wait in the %s kernels gave up (a staging copy did not land); the "
+                            "results since the last check are invalid" % (what or "device check", " and ".join(kinds)))
+
+
 def misfit(data: torch.Tensor, syn: torch.Tensor, adstf: torch.Tensor, nshots: int, nrec: int, nt: int, dt: float,
            stream=None) -> torch.Tensor:
     """Per-shot L2 misfit (FP64) and adjoint source (fwi_misfit)."""

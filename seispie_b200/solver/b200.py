@@ -435,7 +435,7 @@ class b200:
                     if mode == FWI_SPIN:
                         self.obs_y = DeviceArray(b.obs[1], None, self.stream)
         self._write_output_traces(isrc)
-        self.stream.synchronize()
+        engine.check_device(self.stream, "run_forward")
 
     def _forward_exact_shot(self, mode, isrc):
         """Forward of one shot set with the exact adjoint's checkpoints kept."""
@@ -616,6 +616,7 @@ class b200:
                     b.run(d, True, 0, nt)
         self._adjoint_state, self._adj_src = {}, {}
         self._illum_valid = all(self._exact(m) for m in self.modes)
+        engine.check_device(self.stream, "run_adjoint")
 
     def run_kernel(self, adj):
         """solver.py:332-404, all shots of this process batched: forward with
@@ -655,6 +656,8 @@ class b200:
                         b.clear()
                         b.run(d, True, 0, nt)
                 del b
+        # every kernel of this gradient has run its bounded waits to the end, or the call fails here
+        engine.check_device(self.stream, "run_kernel")
         if self.mpi:
             misfit = self._mpi_sum_misfit(misfit)
             self._mpi_sum_kernels()

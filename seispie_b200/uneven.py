@@ -124,6 +124,11 @@ class UnevenBatch:
         for inst, m, b, d in self.items:
             b.cur = d.cur
 
+    def check(self) -> None:
+        """Wait for the work queued so far and raise FwiError if a bounded
+        wait in a step kernel gave up (engine.check_device)."""
+        engine.check_device(None, "UnevenBatch")
+
     def capture(self):
         """Record clear + every step of every group into one CUDA graph."""
         self.clear()

@@ -103,3 +103,10 @@ def test_check_raises_with_message():
     lib = _lib.load()
     with pytest.raises(_lib.FwiError, match="pitch"):
         _lib.check(lib.fwi_run(ctypes.byref(_batch(pitch=18)), 0, 0, 1, None), "fwi_run")
+
+
+def test_wait_limit_rejects_negative_before_any_cuda_call():
+    lib = _lib.load()
+    assert lib.fwi_set_wait_limit(-5) == -1
+    code, msg = _err()
+    assert code == -1 and "polls" in msg

@@ -67,6 +67,6 @@ def test_uneven_batch_vs_fp64_oracle():
     ub.prepare()
     ub.clear()
     ub.run()
-    torch.cuda.synchronize()
+    ub.check()
     for k, inst in enumerate(insts):
         assert oracle_error(inst, ub.traces(k), inst.nt) < 1e-5, k
