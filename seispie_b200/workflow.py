@@ -21,33 +21,57 @@ from os import getcwd, makedirs, path
 from time import time
 
 
-def parse_config(workdir: str, config_file: str):
-    """sprun:10-42."""
+# Sections a child configuration inherits from its parent (the set sprun
+# merges, scripts/sprun:24).
+INHERITED_SECTIONS = ("workflow", "slurm", "preprocess", "solver", "postprocess", "optimize", "path")
+
+
+def _adopt(section: str, value: str, parent_rel: str) -> str:
+    """A parent's value as the child sees it: entries of [path] are written
+    relative to the parent's directory, so they are rebased onto it, except
+    'no' (a path switched off); every other value is taken as written."""
+    if section == "path" and value != "no":
+        return parent_rel + "/" + value
+    return value
+
+
+def merge_configs(child: dict, parent: dict, parent_rel: str) -> dict:
+    """child with every key it does not set taken from parent (dicts of
+    sections of strings), for the inherited sections only."""
+    out = {sec: dict(keys) for sec, keys in child.items()}
+    for sec in INHERITED_SECTIONS:
+        for key, value in parent.get(sec, {}).items():
+            out.setdefault(sec, {}).setdefault(key, _adopt(sec, value, parent_rel))
+    return out
+
+
+def _read(config_path: str) -> dict:
+    cp = ConfigParser()
+    cp.read(config_path)
+    return {sec: dict(cp[sec]) for sec in cp.sections()}
+
+
+def _resolve(workdir: str, config_file: str) -> dict:
+    """The configuration of workdir with its inheritance chain applied."""
     config_path = path.join(workdir, config_file)
-    if not path.exists(workdir) or not path.exists(config_path):
+    if not path.isdir(workdir) or not path.exists(config_path):
         raise FileNotFoundError(config_path)
-    config = ConfigParser()
-    config.read(config_path)
-    if "inherit" in config["workflow"]:
-        parent_name = config["workflow"]["inherit"]
-        parent, _ = parse_config(workdir + "/../" + parent_name, config_file)
-        for section in ["workflow", "slurm", "preprocess", "solver", "postprocess", "optimize", "path"]:
-            if section not in parent:
-                continue
-            if section not in config:
-                config[section] = parent[section]
-                if section == "path":
-                    for key in config[section]:
-                        if config[section][key] != "no":
-                            config[section][key] = "../" + parent_name + "/" + config[section][key]
-            else:
-                for key in parent[section]:
-                    if key not in config[section]:
-                        if section == "path" and parent[section][key] != "no":
-                            config[section][key] = "../" + parent_name + "/" + parent[section][key]
-                        else:
-                            config[section][key] = parent[section][key]
-    return config, workdir
+    cfg = _read(config_path)
+    parent = cfg.get("workflow", {}).get("inherit")
+    if parent:
+        cfg = merge_configs(cfg, _resolve(path.join(workdir, "..", parent), config_file), "../" + parent)
+    return cfg
+
+
+def parse_config(workdir: str, config_file: str):
+    """config.ini of workdir as sprun reads it (scripts/sprun:10-42):
+    ``[workflow] inherit = parent`` takes every key the file does not set
+    from ../parent/config_file (itself resolved the same way), with the
+    parent's paths rebased onto its directory.  Returns (ConfigParser,
+    workdir); its sections are what the modules receive as ``.config``."""
+    cp = ConfigParser()
+    cp.read_dict(_resolve(workdir, config_file))
+    return cp, workdir
 
 
 class _stub:
@@ -131,25 +155,24 @@ class inversion:
 WORKFLOWS = dict(forward=forward, adjoint=adjoint, inversion=inversion)
 
 
+def resolve_paths(path_section, workdir: str) -> dict:
+    """Absolute paths of the [path] entries that are not switched off."""
+    return {key: path.join(workdir, value) for key, value in path_section.items() if value != "no"}
+
+
 def setup(config, workdir, mpi=None):
-    """sprun:55-89; returns the workflow after running it."""
-    path_dict = {}
-    for d in config["path"]:
-        if config["path"][d] != "no":
-            path_dict[d] = path.join(workdir, config["path"][d])
-    if not path.exists(path_dict["output"]):
-        makedirs(path_dict["output"])
-    mode = config["workflow"]["mode"]
-    wf = WORKFLOWS[mode]()
-    wf.dict = path_dict
-    wf.mpi = mpi
+    """Run the workflow named by [workflow] mode (scripts/sprun:55-89): every
+    module it lists is created from its section's ``method`` and given
+    ``.config``, ``.path`` and ``.mpi`` before ``setup(workflow)``.  Returns
+    the workflow after it ran."""
+    paths = resolve_paths(config["path"], workdir)
+    makedirs(paths["output"], exist_ok=True)
+    wf = WORKFLOWS[config["workflow"]["mode"]]()
+    wf.dict, wf.mpi = paths, mpi
     wf.setup()
     for section in wf.modules:
-        method = config[section]["method"] if "method" in config[section] else "default"
-        module = load_module(section, method)
-        module.config = config[section]
-        module.path = path_dict
-        module.mpi = mpi
+        module = load_module(section, config[section].get("method", "default"))
+        module.config, module.path, module.mpi = config[section], paths, mpi
         module.setup(wf)
         setattr(wf, section, module)
     wf.run()

@@ -134,3 +134,17 @@ def test_plugin_shot_sharding_and_kernel_sum_two_ranks_gloo():
     for _, _, ks, m in res:
         assert m == total
         assert ks == [total * (f + 1) for f in range(7)]
+
+
+def test_merge_rule_edges():
+    """A section the child lacks comes whole from the parent (paths
+    rebased), sections outside the inherited set are not inherited, a
+    child's own value wins, 'no' stays 'no'."""
+    from seispie_b200.workflow import merge_configs
+    parent = {"path": {"model_true": "mt", "traces": "no"}, "solver": {"nt": "10", "dt": "1e-3"},
+              "custom": {"x": "1"}}
+    child = {"workflow": {"inherit": "p"}, "solver": {"nt": "20"}}
+    out = merge_configs(child, parent, "../p")
+    assert out["path"] == {"model_true": "../p/mt", "traces": "no"}
+    assert out["solver"] == {"nt": "20", "dt": "1e-3"}
+    assert "custom" not in out and out["workflow"] == {"inherit": "p"}
