@@ -27,13 +27,14 @@ import numpy as np
 
 def write_case(root: str, nx: int, nz: int, shots: int, nrec: int, nt: int, niter: int, sigma: int, sae: int,
                h: float = 10.0, dt: float = 1e-3, square: int = 64, amp: float = 0.08, board=None,
-               method: str = "lbfgs", optimize_extra: str = "", perturb: str = "both"):
+               method: str = "lbfgs", optimize_extra: str = "", perturb: str = "both", invert: str = "mu"):
     """board: perturbation pattern in [-1, 1] ([nx, nz]; default the
     checkerboard of `square`-cell squares); perturb: "both" (vp and vs), "vs"
     (vs only) or "mu" (vs with vp adjusted so that lambda keeps its starting
     value: the model error is then in the inverted parameter mu alone);
     method / optimize_extra: the [optimize] method and further keys
-    (lines) of the inversion config."""
+    (lines) of the inversion config; invert: the solver's model variables
+    (mu, or vp_vs).  Returns the true (vp, vs, mu)."""
     from .io import write_model
     i, j = np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij")
     vp0 = 3000.0 + 300.0 * (j / (nz - 1) - 0.5)
@@ -70,10 +71,10 @@ def write_case(root: str, nx: int, nz: int, shots: int, nrec: int, nt: int, nite
                 % (sae, sigma))
     os.makedirs(os.path.join(root, "inverse"), exist_ok=True)
     with open(os.path.join(root, "inverse", "config.ini"), "w") as f:
-        f.write("[workflow]\nmode = inversion\ninherit = adjoint\n\n[optimize]\nniter = %d\nmethod = %s\n"
-                "ls_step = 10\nls_step_max = 0.5\nls_step_init = 0.05\nls_thresh = 1.2\nlbfgs_mem = 5\n%s\n"
-                "[path]\noutput = output\n" % (niter, method, optimize_extra))
-    return 2600.0 * true["vs"] ** 2
+        f.write("[workflow]\nmode = inversion\ninherit = adjoint\n\n[solver]\ninvert = %s\n\n[optimize]\nniter = %d\n"
+                "method = %s\nls_step = 10\nls_step_max = 0.5\nls_step_init = 0.05\nls_thresh = 1.2\nlbfgs_mem = 5\n"
+                "%s\n[path]\noutput = output\n" % (invert, niter, method, optimize_extra))
+    return true["vp"], true["vs"], 2600.0 * true["vs"] ** 2
 
 
 def main(argv=None):
@@ -86,10 +87,13 @@ def main(argv=None):
     ap.add_argument("--niter", type=int, default=20)
     ap.add_argument("--sigma", type=int, default=4)
     ap.add_argument("--sae", type=int, default=10)
+    ap.add_argument("--invert", default="vp_vs", choices=["mu", "vp_vs"],
+                    help="model variables: vp_vs (both perturbed velocities) or mu (the reference's)")
     a = ap.parse_args(argv)
     from . import workflow
     root = tempfile.mkdtemp()
-    mu_true = write_case(root, a.nx, a.nz, a.shots, a.nrec, a.nt, a.niter, a.sigma, a.sae)
+    vp_true, vs_true, mu_true = write_case(root, a.nx, a.nz, a.shots, a.nrec, a.nt, a.niter, a.sigma, a.sae,
+                                           invert=a.invert)
     t0 = time.time()
     with contextlib.redirect_stdout(io.StringIO()):
         wf = workflow.main(["--workdir", os.path.join(root, "inverse")])
@@ -100,13 +104,16 @@ def main(argv=None):
     t = [h["t"] for h in hist]
     t90 = next((t[k] for k in range(len(mis)) if mis[k] <= 0.1 * mis[0]), None)
     mu = wf.solver.mu.copy_to_host()
-    mu_init = None
-    err = float(np.linalg.norm(mu - mu_true) / np.linalg.norm(mu_true))
+    vp, vs = (x[:, : a.nz].reshape(-1).cpu().numpy() for x in wf.solver._velocities())
+
+    def rel(x, y):
+        return float(np.linalg.norm(x - y) / np.linalg.norm(y))
+
     line = {"workload": "psv_inversion_%dx%d_shots%d_nt%d_lbfgs%d" % (a.nx, a.nz, a.shots, a.nt, a.niter),
-            "cells_per_gradient": 2 * a.shots * a.nx * a.nz * a.nt, "total_s": total,
+            "invert": a.invert, "cells_per_gradient": 2 * a.shots * a.nx * a.nz * a.nt, "total_s": total,
             "s_per_iteration": (t[-1] - t[0]) / max(1, len(t) - 1), "misfit": mis, "t": t,
             "misfit_ratio_final": mis[-1] / mis[0], "time_to_90pct_drop_s": t90,
-            "final_mu_rel_err_vs_true": err, "line_search_statuses": "see misfits", "mu_init": mu_init}
+            "final_rel_err_vs_true": {"mu": rel(mu, mu_true), "vp": rel(vp, vp_true), "vs": rel(vs, vs_true)}}
     print(json.dumps(line))
     return line
 

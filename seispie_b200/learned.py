@@ -102,8 +102,8 @@ def run_inversion(root: str, nx: int, nz: int, shots: int, nt: int, niter: int, 
     true mu of the case)."""
     from . import workflow
     from .inversion_bench import write_case
-    mu_true = write_case(root, nx, nz, shots, nrec or max(16, nx // 4), nt, niter, sigma, 10, board=board, amp=amp,
-                         method=method, optimize_extra=extra, perturb=perturb)
+    _, _, mu_true = write_case(root, nx, nz, shots, nrec or max(16, nx // 4), nt, niter, sigma, 10, board=board,
+                               amp=amp, method=method, optimize_extra=extra, perturb=perturb)
     t0 = time.time()
     with contextlib.redirect_stdout(io.StringIO()):
         wf = workflow.main(["--workdir", os.path.join(root, "inverse")])

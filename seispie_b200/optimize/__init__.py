@@ -43,7 +43,7 @@ class base:
             self.g_new, misfit, self.m_new = solver.compute_gradient_device()
             if head:
                 if i > 0:
-                    solver.export_field(self.m_new.cpu().numpy(), "mu", i - 1)
+                    solver.export_model(self.m_new, i - 1)
                 else:
                     ref = misfit
                 misfits.append(misfit / ref)
@@ -60,10 +60,7 @@ class base:
         self.history.append(dict(iteration=niter, misfit=misfit, t=time() - start))
         if head:
             misfits.append(misfit / ref)
-            m_new = np.zeros(solver.nx * solver.nz, dtype="float32")
-            solver.mu.copy_to_host(m_new, solver.stream)
-            solver.stream.synchronize()
-            solver.export_field(m_new, "mu", niter)
+            solver.export_model(solver.model_vector_device(), niter)
             print("Misfits:")
             for m in misfits:
                 print("  %.4f" % m)

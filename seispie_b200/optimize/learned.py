@@ -30,6 +30,8 @@ from . import lbfgs
 class lbfgs_learned(lbfgs):
     def setup(self, workflow):
         super().setup(workflow)
+        if getattr(self.solver, "invert", "mu") != "mu":
+            raise ValueError("the learned preconditioner maps mu gradients: use invert = mu")
         self.pre = None
         path = self.config.get("unet_weights", "") if hasattr(self.config, "get") else ""
         if path:

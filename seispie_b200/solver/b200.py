@@ -113,6 +113,11 @@ class b200:
         self.tile = int(self.config.get("tile", 0))
         self.batch_memory = float(self.config.get("batch_memory_gb", 0)) * 2 ** 30
         self.kernel_rho = self.config.get("kernel_rho", "no") == "yes"
+        # model variables of the GPU optimizers: mu alone, as the reference inverts (fd2d.py:442-443),
+        # or vp and vs together
+        self.invert = self.config.get("invert", "mu")
+        if self.invert not in ("mu", "vp_vs"):
+            raise ValueError("invert = %r: mu or vp_vs" % self.invert)
         self.model = None
 
     def _ctx(self):
@@ -707,20 +712,74 @@ class b200:
         return out_k, misfit, out_m
 
     def compute_gradient_device(self):
-        """compute_gradient without leaving the device: (smoothed k_mu, misfit,
-        mu) as float32 CUDA vectors of npt (the GPU optimizers' entry)."""
+        """compute_gradient without leaving the device: (smoothed gradient,
+        misfit, model) as float32 CUDA vectors (the GPU optimizers' entry).
+        invert = mu: k_mu and mu, npt each.  invert = vp_vs: [vp; vs] (2 npt)
+        and its gradient from the exact kernels by the chain rule,
+        dchi/dvp = 2 rho vp k_lam and dchi/dvs = 2 rho vs (k_mu - 2 k_lam),
+        each smoothed like k_mu."""
         misfit, kernel, model = self.run_kernel(1)
         with self._ctx():
-            g = kernel.tensor.reshape(-1).clone()
-            m = model._flat().clone()
+            if self.invert == "mu":
+                g = kernel.tensor.reshape(-1).clone()
+                m = model._flat().clone()
+            else:
+                nz = self.nz
+                rho = self.model.rho.double()
+                vp, vs = self._velocities()
+                g_vp = 2.0 * rho * vp.double() * self.k_lam_f64
+                g_vs = 2.0 * rho * vs.double() * (self.k_mu_f64 - 2.0 * self.k_lam_f64)
+                g = torch.cat([engine.smooth(g_vp, self.grid, self.sigma, self.stream),
+                               engine.smooth(g_vs, self.grid, self.sigma, self.stream)])
+                m = torch.cat([vp[:, :nz].reshape(-1), vs[:, :nz].reshape(-1)]).clone()
         self.stream.synchronize()
         return g, misfit, m
 
-    def update_model_device(self, mu: torch.Tensor):
-        """update_model from a float32 CUDA vector of npt."""
+    def _velocities(self):
+        """vp, vs ([nx, pitch] float32) of the current lam, mu, rho
+        (lm2vps, fd2d.py:36-44)."""
+        vp, vs = self.model.lam.clone(), self.model.mu.clone()
+        engine.check(engine._lib.load().fwi_lm2vps(engine.ptr(vp), engine.ptr(vs), engine.ptr(self.model.rho),
+                                                   vp.numel(), engine.stream_handle(self.stream)), "fwi_lm2vps")
+        return vp, vs
+
+    def update_model_device(self, m: torch.Tensor):
+        """update_model from a float32 CUDA vector: mu (npt), or [vp; vs]
+        (2 npt) converted to lam and mu on the device (vps2lm,
+        fd2d.py:21-33)."""
         torch.cuda.current_stream().synchronize()
+        nx, nz, npt = self.nx, self.nz, self.nx * self.nz
         with self._ctx():
-            self.model.mu[:, : self.nz].copy_(mu.reshape(self.nx, self.nz))
+            if self.invert == "mu":
+                self.model.mu[:, :nz].copy_(m.reshape(nx, nz))
+            else:
+                self.model.lam[:, :nz].copy_(m[:npt].reshape(nx, nz))
+                self.model.mu[:, :nz].copy_(m[npt:].reshape(nx, nz))
+                engine.check(engine._lib.load().fwi_vps2lm(engine.ptr(self.model.lam), engine.ptr(self.model.mu),
+                                                           engine.ptr(self.model.rho), self.model.lam.numel(),
+                                                           engine.stream_handle(self.stream)), "fwi_vps2lm")
+
+    def export_model(self, m, it):
+        """Write an optimizer model vector as the reference's model files:
+        mu, or vp and vs (fd2d.py:254-261)."""
+        m = m.detach().float().cpu().numpy() if isinstance(m, torch.Tensor) else np.asarray(m, np.float32)
+        npt = self.nx * self.nz
+        if self.invert == "mu":
+            self.export_field(m[:npt], "mu", it)
+        else:
+            self.export_field(m[:npt], "vp", it)
+            self.export_field(m[npt:], "vs", it)
+
+    def model_vector_device(self):
+        """The optimizer's model vector of the current model (float32 CUDA)."""
+        with self._ctx():
+            if self.invert == "mu":
+                m = self.model.mu[:, : self.nz].reshape(-1).clone()
+            else:
+                vp, vs = self._velocities()
+                m = torch.cat([vp[:, : self.nz].reshape(-1), vs[:, : self.nz].reshape(-1)])
+        self.stream.synchronize()
+        return m
 
     def smooth(self, data):
         """fd2d.py:349-352: Gaussian smoothing of a device field (FP64
