@@ -78,6 +78,10 @@ def parse():
     ap.add_argument("--profile-case", action="store_true",
                     help="only run a few forward steps (for ncu captures of the step kernel)")
     ap.add_argument("--autotune", action="store_true", help="time every tile variant and report the best")
+    ap.add_argument("--overlap", type=int, default=0, choices=[0, 1],
+                    help="1: recompute segment s-1 on a second stream while segment s is transposed")
+    ap.add_argument("--overlap-ctas", type=int, default=0,
+                    help="with --overlap: resident CTAs per SM of the recomputing step (0: all that fit)")
     ap.add_argument("--shard", action="store_true",
                     help="split the --shots shots over the ranks (strong scaling) instead of --shots per rank")
     ap.add_argument("--gradient", default="exact", choices=["exact", "reference"],
@@ -338,9 +342,11 @@ def main():
         # per-step stores of the last steps kept from the forward sweep: the longest tail that fits
         # 90 % of the free HBM with the checkpoints, segment stores, wavefields and traces
         free, _ = torch.cuda.mem_get_info(dev)
-        tail = max_tail_bytes(nt, FWI_PSV, nshots, m_init.grid, 0.9 * free, a.nrec)
-        ea = ExactAdjoint(m_init, nt, sid, lambda s: mine[s], nshots, stf, rid, tile=a.tile, tail_memory=tail)
-        checkpointing = {"segment": ea.K, "checkpoints": ea.nseg, "stored_tail_steps": ea.tail}
+        tail = max_tail_bytes(nt, FWI_PSV, nshots, m_init.grid, 0.9 * free, a.nrec, overlap=bool(a.overlap))
+        ea = ExactAdjoint(m_init, nt, sid, lambda s: mine[s], nshots, stf, rid, tile=a.tile, tail_memory=tail,
+                          overlap=bool(a.overlap), overlap_ctas=a.overlap_ctas)
+        checkpointing = {"segment": ea.K, "checkpoints": ea.nseg, "stored_tail_steps": ea.tail,
+                         "overlap": ea.overlap, "overlap_ctas": ea.overlap_ctas}
         grads = [torch.empty((nshots, a.nrec, nt), dtype=torch.float32, device=dev) if c != 1 else None
                  for c in range(3)]
         b = ea.fwd

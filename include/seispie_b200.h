@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define FWI_ABI_VERSION 5
+#define FWI_ABI_VERSION 6
 
 /* status codes */
 #define FWI_OK 0
@@ -121,6 +121,10 @@ typedef struct fwi_batch {
     /* Displacement-free batches: row slots of the row-marching kernel's
      * staging ring, 3, 4, 6 or 8 (0 = chosen from the row length). */
     int ring;
+    /* Row-marching step: resident CTAs per SM its grid is sized for (0 =
+     * as many as fit).  A smaller grid leaves room on every SM for another
+     * kernel running concurrently on a second stream. */
+    int ctas_per_sm;
 } fwi_batch;
 
 /* ABI version of the loaded library (FWI_ABI_VERSION). */

@@ -53,37 +53,42 @@ def default_segment(nt: int, mode: int, nshots: int, grid: Grid, budget_bytes: f
     return min(k, nt)
 
 
-def fixed_bytes(nt: int, mode: int, nshots: int, grid: Grid, nrec: int = 0, segment: int | None = None) -> int:
+def fixed_bytes(nt: int, mode: int, nshots: int, grid: Grid, nrec: int = 0, segment: int | None = None,
+                overlap: bool = False) -> int:
     """Upper bound of the device bytes an ExactAdjoint (levels = 1) holds
     besides its stored tail: checkpoints every K steps over all nt steps, one
-    segment of per-step stores, the wavefields of the forward and adjoint
-    batches (ping-pong stress and velocity, displacement where kept) and, per
-    velocity component, the traces, the observed data and the trace
-    gradients.  A stored tail has to fit in what is left."""
+    segment of per-step stores (two with overlap), the wavefields of the
+    forward and adjoint batches (ping-pong stress and velocity, displacement
+    where kept) and, per velocity component, the traces, the observed data
+    and the trace gradients.  A stored tail has to fit in what is left."""
     k = segment or default_segment(nt, mode, nshots, grid)
     field = 4 * nshots * grid.nx * grid.pitch
     state = state_fields(mode, grid)
     per_step = strain_fields(mode) + NV[mode]
     batch = 2 * NS[mode] + 2 * NV[mode] + (state - NS[mode] - NV[mode])
-    return (math.ceil(nt / k) * state + k * per_step + 2 * batch) * field + 3 * 4 * nshots * nrec * nt * NV[mode]
+    segs = 2 if overlap else 1
+    return ((math.ceil(nt / k) * state + segs * k * per_step + 2 * batch) * field
+            + 3 * 4 * nshots * nrec * nt * NV[mode])
 
 
 def max_tail_bytes(nt: int, mode: int, nshots: int, grid: Grid, budget_bytes: float, nrec: int = 0,
-                   segment: int | None = None) -> int:
+                   segment: int | None = None, overlap: bool = False) -> int:
     """Largest stored tail (as ExactAdjoint's tail_memory, in bytes) whose
     ExactAdjoint (levels = 1) fits budget_bytes in all: checkpoints of the
-    steps before the tail, one segment of per-step stores, the tail's
-    per-step stores, both batches' wavefields and the trace arrays (the
-    terms of fixed_bytes).  A longer tail needs fewer checkpoints."""
+    steps before the tail, one segment of per-step stores (two with
+    overlap), the tail's per-step stores, both batches' wavefields and the
+    trace arrays (the terms of fixed_bytes).  A longer tail needs fewer
+    checkpoints."""
     k = segment or default_segment(nt, mode, nshots, grid)
     field = 4 * nshots * grid.nx * grid.pitch
     state = state_fields(mode, grid)
     per_step = strain_fields(mode) + NV[mode]
     batch = 2 * NS[mode] + 2 * NV[mode] + (state - NS[mode] - NV[mode])
     traces = 3 * 4 * nshots * nrec * nt * NV[mode]
+    segs = 2 if overlap else 1
 
     def need(t):
-        return (math.ceil((nt - t) / k) * state + k * per_step + t * per_step + 2 * batch) * field + traces
+        return (math.ceil((nt - t) / k) * state + segs * k * per_step + t * per_step + 2 * batch) * field + traces
 
     lo, hi = 0, nt  # need() grows with t: the largest t with need(t) <= budget
     if need(0) > budget_bytes:
@@ -124,17 +129,26 @@ class ExactAdjoint:
     tail_memory (bytes): HBM the forward sweep may fill with the per-step
     stores of its last steps; those steps are then transposed without being
     recomputed (exactly the same values, so the same gradient), and only the
-    steps before them are checkpointed."""
+    steps before them are checkpointed.
+
+    overlap (levels = 1): two segments of per-step stores; the backward
+    recomputes segment s-1 on a second stream while the transposes of
+    segment s run, so that the two kernels share the SMs (same values, so
+    the same gradient bit for bit); overlap_ctas caps the resident CTAs per
+    SM of the recomputing row-marching step (0: no cap), leaving room for
+    the transposed step's CTAs."""
 
     def __init__(self, model: DeviceModel, nt: int, src_id, isrc_of_shot, nshots: int, stf, rec_id,
                  segment: int | None = None, tile: int = 0, levels: int = 1, sub_segment: int | None = None,
-                 tail_memory: float = 0.0):
+                 tail_memory: float = 0.0, overlap: bool = False, overlap_ctas: int = 0):
         self.model, self.nt, self.nshots = model, int(nt), int(nshots)
         self.rec_id = np.asarray(rec_id, np.int32)
         self.mode = model.mode
         g = model.grid
         if levels not in (1, 2):
             raise ValueError("levels must be 1 or 2")
+        if overlap and levels != 1:
+            raise ValueError("overlap needs levels = 1")
         self.levels = levels
         if levels == 1:
             self.K = segment or default_segment(self.nt, self.mode, self.nshots, g)
@@ -168,6 +182,11 @@ class ExactAdjoint:
             self.seg_e[k] = torch.empty((self.K2,) + shape, dtype=torch.float32, device=dev)
         for c in COMP[self.mode][: NV[self.mode]]:
             self.seg_ds[c] = torch.empty((self.K2,) + shape, dtype=torch.float32, device=dev)
+        self.overlap = bool(overlap) and self.nseg > 1
+        self.overlap_ctas = int(overlap_ctas)
+        if self.overlap:
+            self.seg_e2 = [None if t is None else torch.empty_like(t) for t in self.seg_e]
+            self.seg_ds2 = [None if t is None else torch.empty_like(t) for t in self.seg_ds]
         self.tail_e, self.tail_ds = [None] * 6, [None, None, None]
         if self.tail:
             for k in range(strain_fields(self.mode)):
@@ -245,6 +264,9 @@ class ExactAdjoint:
             adj.set_segment(adesc, self.seg_e, self.seg_ds, t0, n)
             adj.run_transposed(adesc, t0 + n, n)
 
+        if self.overlap:
+            self._backward_overlapped(adj, adesc)
+            return tuple(k)
         if self.tail:
             adj.set_segment(adesc, self.tail_e, self.tail_ds, self.t0, self.tail)
             adj.run_transposed(adesc, self.nt, self.tail)
@@ -268,6 +290,55 @@ class ExactAdjoint:
                 reverse(s0 + jj * self.K2, min(self.K2, n - jj * self.K2))
         fwd.set_segment(self.rdesc, [None] * 6, [None] * 3, 0, 0)
         return tuple(k)
+
+    def _backward_overlapped(self, adj: ShotBatch, adesc) -> None:
+        """The levels = 1 backward with the recomputation one segment ahead
+        on a second stream: segment s-1 is recomputed into one store buffer
+        while the transposes of segment s read the other; a buffer is
+        refilled only after the transposes that read it (CUDA events)."""
+        fwd = self.fwd
+        main = torch.cuda.current_stream() if adj.stream is None else adj.stream
+        side = torch.cuda.Stream(device=self.model.device)
+        side.wait_stream(main)  # the forward sweep and the trace sums
+        bufs = ((self.seg_e, self.seg_ds), (self.seg_e2, self.seg_ds2))
+        freed = [None, None]  # per buffer: event after the last transposes that read it
+
+        def recompute(s):
+            j = s % 2
+            s0, n = s * self.K, min(self.K, self.t0 - s * self.K)
+            with torch.cuda.stream(side):
+                if freed[j] is not None:
+                    side.wait_event(freed[j])
+                for q, t in enumerate(fwd.state_tensors()):
+                    t.copy_(self.ckpt[s, q])
+                fwd.set_segment(self.rdesc, bufs[j][0], bufs[j][1], s0, n)
+                fwd.run(self.rdesc, False, s0, n)
+                ev = torch.cuda.Event()
+                ev.record(side)
+            return ev
+
+        saved = fwd.stream
+        fwd.stream = side
+        self.rdesc.ctas_per_sm = self.overlap_ctas
+        try:
+            ready = recompute(self.nseg - 1)
+            if self.tail:
+                adj.set_segment(adesc, self.tail_e, self.tail_ds, self.t0, self.tail)
+                adj.run_transposed(adesc, self.nt, self.tail)
+            for s in reversed(range(self.nseg)):
+                main.wait_event(ready)
+                ready = recompute(s - 1) if s > 0 else None
+                j = s % 2
+                s0, n = s * self.K, min(self.K, self.t0 - s * self.K)
+                adj.set_segment(adesc, bufs[j][0], bufs[j][1], s0, n)
+                adj.run_transposed(adesc, s0 + n, n)
+                freed[j] = torch.cuda.Event()
+                freed[j].record(main)
+            main.wait_stream(side)
+        finally:
+            fwd.stream = saved
+            self.rdesc.ctas_per_sm = fwd.ctas_per_sm
+            fwd.set_segment(self.rdesc, [None] * 6, [None] * 3, 0, 0)
 
 
 def _pad(t: torch.Tensor, grid: Grid) -> torch.Tensor:

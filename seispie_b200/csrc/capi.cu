@@ -117,6 +117,7 @@ static int check_batch(const fwi_batch *b, int adjoint, int it0, int nsteps) {
         REQUIRE(!rec || b->rec_order, "displacement-free batches that record traces need rec_order");
         REQUIRE(b->ring == 0 || b->ring == 3 || b->ring == 4 || b->ring == 6 || b->ring == 8,
                 "ring must be 0, 3, 4, 6 or 8 (got %d)", b->ring);
+        REQUIRE(b->ctas_per_sm >= 0, "ctas_per_sm must be >= 0 (got %d)", b->ctas_per_sm);
     }
     if (adjoint) {
         REQUIRE(b->sae >= 1, "the adjoint needs adjoint_interval >= 1");

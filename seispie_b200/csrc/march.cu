@@ -770,6 +770,7 @@ int launch_march(const fwi_batch *b, int it, cudaStream_t st) {
     int rc = mode == FWI_SH ? march_choose<FWI_SH>(nthr, a.rl, b->ring, &n, &bytes, &occ)
                             : march_choose<FWI_PSV>(nthr, a.rl, b->ring, &n, &bytes, &occ);
     if (rc) return rc;
+    if (b->ctas_per_sm > 0 && b->ctas_per_sm < occ) occ = b->ctas_per_sm;
     if (mode == FWI_SH) {
         switch (n) {
             case 3: return launch_march_mode<FWI_SH, 3>(a, nthr, bytes, occ, st);

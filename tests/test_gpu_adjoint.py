@@ -348,8 +348,9 @@ def test_spin_exact_gradient_directional_derivatives():
 
 @pytest.mark.parametrize("mode", ["psv", "spin"])
 def test_two_level_checkpointing_is_bit_identical(mode):
-    """Recursive (two-level) checkpointing, and per-step stores kept from the
-    forward sweep for the last steps, produce the same forward values as
+    """Recursive (two-level) checkpointing, per-step stores kept from the
+    forward sweep for the last steps, and the backward that recomputes one
+    segment ahead on a second stream produce the same forward values as
     single-level recomputation, so the gradients are equal exactly."""
     from seispie_b200.adjoint import AcquisitionSetup, ExactAdjoint
     from seispie_b200.engine import Grid, build_model
@@ -372,12 +373,14 @@ def test_two_level_checkpointing_is_bit_identical(mode):
     per_step = (6 + 3 if mode == "spin" else 3 + 2) * 4 * setup.nshots * nx * grid.pitch
     out = []
     for kw in (dict(segment=37), dict(levels=2, segment=50, sub_segment=7),
-               dict(segment=37, tail_memory=61.5 * per_step)):
+               dict(segment=37, tail_memory=61.5 * per_step), dict(segment=37, overlap=True),
+               dict(segment=23, tail_memory=61.5 * per_step, overlap=True)):
         ea = ExactAdjoint(m, nt, setup.src_id, setup.isrc_of_shot, setup.nshots, setup.stf, setup.rec_id, **kw)
         tr = ea.forward()
         out.append((tr, ea.backward(g), ea.illum.clone()))
         if "tail_memory" in kw:
             assert ea.tail == 61 and ea.t0 == nt - 61
+        assert ea.overlap == kw.get("overlap", False)
     (tr1, k1, il1) = out[0]
     assert len(k1) == (6 if mode == "spin" else 3)
     for tr2, k2, _ in out[1:]:
