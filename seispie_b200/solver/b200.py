@@ -239,7 +239,7 @@ class b200:
         if snapshots and self._exact(mode):
             from ..adjoint import fixed_bytes
             # checkpoints, segment stores, both batches' wavefields, traces, data and trace gradients
-            return fixed_bytes(self.nt, mode, 1, g, self.nrec)
+            return fixed_bytes(self.nt, mode, 1, g, self.nrec, overlap=True)
         b = (2 * ns + 3 * nv) * field + 4 * self.nrec * self.nt * nv * 3
         if snapshots:
             b += self.nsa * min(nv, 2) * field * (2 if (mode != FWI_SH and self.kernel_rho) else 1)
@@ -274,9 +274,12 @@ class b200:
                 # of a batch
                 tail = 0.0
                 if self.batch_memory <= 0:
-                    tail = max_tail_bytes(nt, mode, n, self.model.grid, 0.85 * self._free_bytes(), nrec)
+                    tail = max_tail_bytes(nt, mode, n, self.model.grid, 0.85 * self._free_bytes(), nrec,
+                                          overlap=True)
+                # two segments of per-step stores: the next segment is recomputed on a second stream
+                # while this one is transposed
                 ea = ExactAdjoint(self.model, nt, self.src_id, lambda s: -1 if combine else chunk[s], n,
-                                  self._stf(mode), self.rec_id, tile=self.tile, tail_memory=tail)
+                                  self._stf(mode), self.rec_id, tile=self.tile, tail_memory=tail, overlap=True)
                 # the observed traces are stacked into pinned host memory on worker threads while
                 # this thread enqueues the forward sweep, then uploaded on a copy stream that the
                 # misfit waits for

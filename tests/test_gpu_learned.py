@@ -53,3 +53,66 @@ def test_recorded_pairs_and_untrained_network_fallback(tmp_path):
     assert all(b <= a * (1 + 1e-9) for a, b in zip(mis2, mis2[1:]))
     assert mis2[-1] < mis2[0]
     assert os.path.exists(w)
+
+
+def _count_solves(monkeypatch):
+    """Record every misfit evaluation (one forward solve) and gradient
+    (forward + adjoint: two solves) of the b200 solver, with its misfit."""
+    from seispie_b200.solver import b200 as Solver
+    log = []
+    misfit, gradient = Solver.compute_misfit, Solver.compute_gradient_device
+
+    def counted_misfit(self):
+        r = misfit(self)
+        log.append((1, float(r)))
+        return r
+
+    def counted_gradient(self):
+        r = gradient(self)
+        log.append((2, float(r[1])))
+        return r
+
+    monkeypatch.setattr(Solver, "compute_misfit", counted_misfit)
+    monkeypatch.setattr(Solver, "compute_gradient_device", counted_gradient)
+    return log
+
+
+def _solves_to_drop(log, frac):
+    cost = 0
+    for n, m in log:
+        cost += n
+        if m <= (1 - frac) * log[0][1]:
+            return cost
+    return None
+
+
+def test_trained_weights_reach_90pct_drop_with_fewer_solves(tmp_path, monkeypatch):
+    """What the shipped model-error weights (unet_psv_mu_error.npz, with the
+    number of learned iterations stored beside them) gain over plain L-BFGS
+    on a fixed held-out case of their training geometry: a random model
+    (seed 4242), 256 x 128 cells, 16 shots, nt 1500, only mu perturbed (8 %),
+    20 iterations.  Counted in wave solves (a misfit evaluation is one, a
+    gradient two), the learned run reaches a 90 % misfit drop in at most
+    0.75 of the solves plain L-BFGS needs (31 against 53 on a B200), and
+    ends with a smaller model error to the true mu."""
+    from seispie_b200.io import read_field
+    from seispie_b200.learned import ERROR_WEIGHTS, random_board, run_inversion
+    nx, nz, shots, nt, niter = 256, 128, 16, 1500, 20
+    board = random_board(np.random.default_rng(4242), nx, nz)
+    log = _count_solves(monkeypatch)
+    res = {}
+    for label, method, extra in (("plain", "lbfgs", ""),
+                                 ("learned", "lbfgs_learned", "unet_weights = %s\n" % ERROR_WEIGHTS)):
+        log.clear()
+        root = str(tmp_path / label)
+        opt, _, mu_true = run_inversion(root, nx, nz, shots, nt, niter, board, 0.08, method, extra, perturb="mu")
+        _, mu = read_field(os.path.join(root, "inverse", "output", "proc%06d_mu.bin" % niter))
+        mt = np.asarray(mu_true, np.float64).ravel()
+        res[label] = dict(solves=_solves_to_drop(log, 0.9), final=log[-1][1] / log[0][1],
+                          err=float(np.linalg.norm(mu - mt) / np.linalg.norm(mt)),
+                          accepted=getattr(opt, "learned_accepted", 0))
+    plain, learned = res["plain"], res["learned"]
+    assert plain["solves"] is not None and learned["solves"] is not None, res
+    assert learned["accepted"] >= 1, res
+    assert learned["solves"] <= 0.75 * plain["solves"], res
+    assert learned["final"] < plain["final"] and learned["err"] < plain["err"], res

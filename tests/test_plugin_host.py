@@ -130,6 +130,8 @@ def test_exact_adjoint_fixed_bytes():
     # and 2 components x (traces, data, trace gradients)
     want = (78 * 5 + 77 * 5 + 2 * 10) * field + 3 * 4 * 64 * 256 * 6000 * 2
     assert fixed_bytes(6000, FWI_PSV, 64, g, 256) == want
+    # the overlapped backward holds a second segment of stores
+    assert fixed_bytes(6000, FWI_PSV, 64, g, 256, overlap=True) == want + 77 * 5 * field
     # an explicit segment; the spin state is 6 stress + 2 x 3 velocity/displacement fields,
     # a step stores 6 strain terms and 3 divergences, a batch holds 2 x (6 + 3) + 3 fields
     assert fixed_bytes(100, FWI_SPIN, 2, Grid(8, 8, 1.0, 1.0), 0, segment=10) == \
@@ -149,11 +151,16 @@ def test_max_tail_bytes_is_the_longest_tail_that_fits():
     field = 4 * ns * 512 * 512
     k = default_segment(nt, FWI_PSV, ns, g)
 
-    def need(t):
-        return (math.ceil((nt - t) / k) * 5 + k * 5 + t * 5 + 20) * field + 3 * 4 * ns * nrec * nt * 2
+    def need(t, segs=1):
+        return (math.ceil((nt - t) / k) * 5 + segs * k * 5 + t * 5 + 20) * field + 3 * 4 * ns * nrec * nt * 2
 
     for budget in (30e9, 100e9, 160e9):
         t = max_tail_bytes(nt, FWI_PSV, ns, g, budget, nrec) // (5 * field)
         assert 0 < t < nt and need(t) <= budget < need(t + 1)
+        t2 = max_tail_bytes(nt, FWI_PSV, ns, g, budget, nrec, overlap=True) // (5 * field)
+        if need(0, 2) <= budget:
+            assert 0 < t2 < t and need(t2, 2) <= budget < need(t2 + 1, 2)
+        else:  # not even the tail-free overlapped backward fits: no tail
+            assert t2 == 0
     assert max_tail_bytes(nt, FWI_PSV, ns, g, 1e9, nrec) == 0  # nothing fits: no tail
     assert max_tail_bytes(100, FWI_PSV, 1, Grid(8, 8, 1.0, 1.0), 1e12, 0) == 100 * 5 * 4 * 8 * 8
