@@ -125,6 +125,10 @@ typedef struct fwi_batch {
      * as many as fit).  A smaller grid leaves room on every SM for another
      * kernel running concurrently on a second stream. */
     int ctas_per_sm;
+    /* P-SV transposed step (fwi_run_transposed): 0 = tiles of 32 x 64 cells,
+     * two z columns per thread; 1 = tiles of 32 x 32 cells, one column per
+     * thread.  Same adjoint fields bit for bit. */
+    int adj_tile;
 } fwi_batch;
 
 /* ABI version of the loaded library (FWI_ABI_VERSION). */

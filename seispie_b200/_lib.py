@@ -35,7 +35,7 @@ class FwiBatch(ctypes.Structure):
         ("k_lam", _vp), ("k_mu", _vp), ("k_rho", _vp),
         ("seg_e", _vp * 6), ("seg_ds", _vp * 3), ("seg0", ctypes.c_int), ("nseg", ctypes.c_int),
         ("k_nu", _vp), ("k_mnc", _vp), ("k_buoj", _vp), ("rec_order", _vp),
-        ("ring", ctypes.c_int), ("ctas_per_sm", ctypes.c_int),
+        ("ring", ctypes.c_int), ("ctas_per_sm", ctypes.c_int), ("adj_tile", ctypes.c_int),
     ]
 
 

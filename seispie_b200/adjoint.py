@@ -184,6 +184,7 @@ class ExactAdjoint:
             self.seg_ds[c] = torch.empty((self.K2,) + shape, dtype=torch.float32, device=dev)
         self.overlap = bool(overlap) and self.nseg > 1
         self.overlap_ctas = int(overlap_ctas)
+        self.adj_tile = 0  # P-SV transposed step: 0 = 32 x 64 tiles, 1 = 32 x 32 tiles (same values)
         if self.overlap:
             self.seg_e2 = [None if t is None else torch.empty_like(t) for t in self.seg_e]
             self.seg_ds2 = [None if t is None else torch.empty_like(t) for t in self.seg_ds]
@@ -251,6 +252,7 @@ class ExactAdjoint:
                 g = g_traces[c].to(torch.float32).contiguous()
                 stf[c] = engine.trace_suffix_sum(g, torch.empty_like(g)).reshape(-1)
         adj = ShotBatch(self.model, self.nshots, self.nt, self.rec_id)
+        adj.adj_tile = self.adj_tile
         adj.clear()
         inj = adjoint_injection_lists(self.nshots, self.rec_id) if len(self.rec_id) else None
         adesc = adj.desc(inj=inj, stf=stf, record=False, kernels=k)

@@ -305,6 +305,7 @@ int fwi_run_transposed(fwi_batch *b, int it_hi, int nsteps, void *stream) {
     for (int k = 0; k < ne; k++) stores = stores && b->seg_e[k];
     REQUIRE(stores, "fwi_run_transposed: the segment stores seg_e / seg_ds are required");
     REQUIRE(b->k_mu, "fwi_run_transposed: k_mu is required");
+    REQUIRE(b->adj_tile == 0 || b->adj_tile == 1, "fwi_run_transposed: adj_tile must be 0 or 1 (got %d)", b->adj_tile);
     if (b->inj_ptr) {
         REQUIRE(b->inj_cell && b->inj_row, "inj_cell and inj_row are required with inj_ptr");
         REQUIRE(b->stf[cx] && (b->mode == FWI_SH || b->stf[2]), "fwi_run_transposed: trace gradients (stf) missing");

@@ -1560,6 +1560,462 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : MODE == FWI_PSV
     cluster.sync();  // keep this CTA's shared memory alive until every rank has read it
 }
 
+// ------------------------------------------------ exact adjoint, wide P-SV tile
+//
+// The P-SV transposed step of adjoint_kernel with each lane owning two
+// adjacent z columns (float2 loads and stores) of a 32 x 64 tile: half the
+// address, mask and loop work per cell, a 14 % velocity halo instead of
+// 20 %, and a stress region 1.34 times the interior instead of 1.48.  The
+// forward strain and divergence are read straight from HBM (pointwise, once)
+// instead of being staged, which keeps two CTAs per SM.  Same arithmetic per
+// cell as adjoint_kernel<FWI_PSV> (the adjoint fields agree bit for bit);
+// the gradient terms are summed over the cluster's CTAs in rank order as
+// there.
+
+struct WideTile {
+    static constexpr int TX = 32, TZ = 64, SX = TX + 6, SZ = TZ + 8, VX = TX + 3, RVZ = TZ + 3;
+    static constexpr int RPW = TX / (kThreads / 32);
+    static constexpr int FS = (SX * SZ + 31) / 32 * 32, FV = (VX * SZ + 31) / 32 * 32;
+    static constexpr int NS = 3, NV = 2, NK = 3, NINJ = 2;
+    // sig~ (turned into t in place), v~ (turned into b v~'), lam and mu of
+    // the stress region, dt/rho and sponge of the velocity region, the
+    // injection list and three mbarriers (model, sig~, v~)
+    static constexpr int V_OFF = NS * FS, L_OFF = V_OFF + NV * FV, P_OFF = L_OFF + 2 * FS;
+    static constexpr int LIST_OFF = P_OFF + 2 * FV;
+    static constexpr int LIST = kThreads * (1 + NINJ) + 8;
+    static constexpr int BAR_OFF = (LIST_OFF + LIST + 1) / 2 * 2;
+    static constexpr size_t bytes = sizeof(float) * (size_t)(BAR_OFF + 8);
+    static constexpr uint32_t sig_bytes = 4u * NS * SX * SZ;
+    static constexpr uint32_t vel_bytes = 4u * NV * VX * SZ;
+    static constexpr uint32_t model_bytes = 4u * (2 * SX * SZ + 2 * VX * SZ);
+    static_assert(RPW * (kThreads / 32) == TX && 2 * 32 == TZ, "a warp spans the tile's z extent, two columns a lane");
+    static_assert(NK * TX * TZ <= L_OFF, "gradient terms overlay the per-shot buffers");
+    static_assert(FS % 4 == 0 && FV % 4 == 0 && SZ % 4 == 0, "float4 / float2 alignment of the regions");
+};
+
+struct WideMaps {
+    CUtensorMap sig[3];  // sig~, stress region box
+    CUtensorMap vel[2];  // v~, velocity region box
+    CUtensorMap lm[2];   // lam, mu; stress region box
+    CUtensorMap vp[2];   // dt/rho, sponge; velocity region box
+};
+
+// One injection entry per thread: its location in the staged v~ (or -1)
+// and its u~ values (adj_fetch for the wide tile).
+__device__ __forceinline__ void wide_fetch(const AdjArgs &a, int base, int p1, int x0, int z0, int &loc,
+                                           float (&val)[2]) {
+    using T = WideTile;
+    const int e = base + (int)threadIdx.x;
+    loc = -1;
+    val[0] = val[1] = 0.f;
+    if (e < p1) {
+        const int k = a.inj_cell[e];
+        const int gx = fdiv(k, a.divnz), gz = k - gx * a.nz;
+        const int rx = gx - (x0 - 1), rz = gz - (z0 - 1);
+        if (rx >= 0 && rx < T::VX && rz >= 0 && rz < T::RVZ) {
+            loc = rx * T::SZ + rz + 3;
+            const long long src = (long long)a.inj_row[e] * a.nt + a.it;
+            val[0] = a.g[0][src];
+            val[1] = a.g[1][src];
+        }
+    }
+}
+
+__device__ __forceinline__ void wide_apply(float *sV, int n, const int *sLoc, const float *sVal, float dt) {
+    if (threadIdx.x != 0) return;
+    for (int q = 0; q < n; q++) {
+        sV[sLoc[q]] += dt * sVal[q];
+        sV[WideTile::FV + sLoc[q]] += dt * sVal[kThreads + q];
+    }
+}
+
+__device__ __forceinline__ float2 ld2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
+__device__ __forceinline__ void st2(float *p, float x, float y) { *reinterpret_cast<float2 *>(p) = make_float2(x, y); }
+
+__global__ void __launch_bounds__(kThreads, 2)
+    adjoint_wide_kernel(const __grid_constant__ AdjArgs a, const __grid_constant__ WideMaps m) {
+    using T = WideTile;
+    constexpr int TX = T::TX, TZ = T::TZ, SX = T::SX, SZ = T::SZ, RVZ = T::RVZ, FS = T::FS, FV = T::FV;
+    constexpr int RPW = T::RPW;
+    extern __shared__ __align__(128) float smem[];
+    float *sS = smem, *sV = smem + T::V_OFF, *sL = smem + T::L_OFF, *sP = smem + T::P_OFF;
+    int *sLoc = reinterpret_cast<int *>(smem + T::LIST_OFF);
+    float *sVal = reinterpret_cast<float *>(sLoc + kThreads);
+    int *sWarp = reinterpret_cast<int *>(sVal + T::NINJ * kThreads);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + T::BAR_OFF);  // model, sig~, v~
+    cg::cluster_group cluster = cg::this_cluster();
+    const int crank = (int)cluster.block_rank(), csize = (int)cluster.num_blocks();
+
+    const int tid = threadIdx.x, lane = tid & 31, ix0 = (tid >> 5) * RPW;
+    const int z0 = blockIdx.x * TZ, x0 = blockIdx.y * TX;
+    const int nx = a.nx, nz = a.nz, pitch = a.pitch, nshots = a.nshots;
+    const int gz = z0 + 2 * lane, col = 2 * lane + 4;  // this lane's columns: gz and gz + 1
+    const bool zin0 = gz < nz, zin1 = gz + 1 < nz;
+    const float dt = a.dt, cx1 = a.cx1, cx2 = a.cx2, cz1 = a.cz1, cz2 = a.cz2;
+    // z masks of the two columns: (D+)^T taps gz-2..gz+1, (D-)^T taps
+    // gz-1..gz+2; all ones (and skipped) unless the tile reaches a z edge
+    const bool zedge = !(z0 >= 3 && z0 + TZ + 4 <= nz);
+    float pz[2][4], mz[2][4];
+#pragma unroll
+    for (int e = 0; e < 2; e++)
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+            const int kp = gz + e - 2 + d, km = gz + e - 1 + d;
+            pz[e][d] = (kp >= 1 && kp < nz - 2) ? 1.f : 0.f;
+            mz[e][d] = (km >= 2 && km < nz - 2) ? 1.f : 0.f;
+        }
+
+    auto issue_sig = [&](int shot) {
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        mbar_expect_tx(&bar[1], T::sig_bytes);
+#pragma unroll
+        for (int f = 0; f < T::NS; f++) tma_load_3d(sS + f * FS, &m.sig[f], z0 - 4, x0 - 3, shot, &bar[1]);
+    };
+    auto issue_vel = [&](int shot) {
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        mbar_expect_tx(&bar[2], T::vel_bytes);
+#pragma unroll
+        for (int q = 0; q < T::NV; q++) tma_load_3d(sV + q * FV, &m.vel[q], z0 - 4, x0 - 1, shot, &bar[2]);
+    };
+    if (tid == 0) {
+#pragma unroll
+        for (int b = 0; b < 3; b++) mbar_init(&bar[b], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+        mbar_expect_tx(&bar[0], T::model_bytes);
+#pragma unroll
+        for (int f = 0; f < 2; f++) tma_load_2d(sL + f * FS, &m.lm[f], z0 - 4, x0 - 3, &bar[0]);
+#pragma unroll
+        for (int p = 0; p < 2; p++) tma_load_2d(sP + p * FV, &m.vp[p], z0 - 4, x0 - 1, &bar[0]);
+        if (crank < nshots) {
+            issue_sig(crank);
+            issue_vel(crank);
+        }
+    }
+
+    float2 gk[T::NK][RPW];
+#pragma unroll
+    for (int k = 0; k < T::NK; k++)
+#pragma unroll
+        for (int q = 0; q < RPW; q++) gk[k][q] = make_float2(0.f, 0.f);
+
+    // the next shot's injection range and (one per thread) entries, fetched a shot ahead
+    int nx_loc = -1, np0 = 0, np1 = 0;
+    float nx_val[2];
+    auto prefetch_entries = [&](int shot) {
+        np0 = a.inj_ptr ? a.inj_ptr[shot] : 0;
+        np1 = a.inj_ptr ? a.inj_ptr[shot + 1] : 0;
+        if (np1 - np0 <= kThreads) wide_fetch(a, np0, np1, x0, z0, nx_loc, nx_val);
+    };
+    if (crank < nshots) prefetch_entries(crank);
+    int i = 0;
+    for (int shot = crank; shot < nshots; shot += csize, i++) {
+        const long long soff = (long long)shot * nx * pitch;
+        const int p0 = np0, p1 = np1;
+        // forward divergence of the interior cells (pointwise, straight from HBM)
+        float2 dsv[2][RPW];
+#pragma unroll
+        for (int q = 0; q < RPW; q++) {
+            const int gx = x0 + ix0 + q;
+            const bool in = zin0 && gx < nx;
+            const long long g = soff + (long long)gx * pitch + gz;
+#pragma unroll
+            for (int c = 0; c < 2; c++) dsv[c][q] = in ? ld2(a.dsf[c] + g) : make_float2(0.f, 0.f);
+        }
+        const bool single = p1 - p0 <= kThreads;
+        int n_in = 0;
+        if (single && p1 > p0) n_in = adj_compact<FWI_PSV>(nx_loc, nx_val, sLoc, sVal, sWarp);
+
+        // sig~ of the interior cells into registers (t overwrites it)
+        bool ok = mbar_wait(&bar[1], i & 1);
+        if (i == 0) ok = mbar_wait(&bar[0], 0) && ok;
+        float2 sg[3][RPW];
+#pragma unroll
+        for (int f = 0; f < 3; f++)
+#pragma unroll
+            for (int q = 0; q < RPW; q++) sg[f][q] = ld2(sS + f * FS + (ix0 + q + 3) * SZ + col);
+        if (__syncthreads_or(!ok)) {  // block-uniform decision
+            if (tid == 0) atomicExch(&g_device_status, 1);
+            mbar_wait(&bar[1], i & 1);
+            mbar_wait(&bar[2], i & 1);
+            if (i == 0) mbar_wait(&bar[0], 0);
+            break;
+        }
+        // t = dt S^T sig~ in place over the whole stress region, four cells at a time
+        for (int c = tid; c < SX * (SZ / 4); c += kThreads) {
+            float4 *s4 = reinterpret_cast<float4 *>(sS) + c;
+            const float4 *l4 = reinterpret_cast<const float4 *>(sL) + c;
+            constexpr int F4 = FS / 4;
+            const float4 l = l4[0], mu = l4[F4];
+            float4 xx = s4[0], zz = s4[F4], xz = s4[2 * F4];
+            auto t3 = [&](float lc, float mc, float &sxx, float &szz, float &sxz) {
+                const float l2m = lc + 2.f * mc, p = sxx, r = szz;
+                sxx = dt * (l2m * p + lc * r);
+                szz = dt * (lc * p + l2m * r);
+                sxz = dt * (mc * sxz);
+            };
+            t3(l.x, mu.x, xx.x, zz.x, xz.x);
+            t3(l.y, mu.y, xx.y, zz.y, xz.y);
+            t3(l.z, mu.z, xx.z, zz.z, xz.z);
+            t3(l.w, mu.w, xx.w, zz.w, xz.w);
+            s4[0] = xx;
+            s4[F4] = zz;
+            s4[2 * F4] = xz;
+        }
+        // v~ of this shot; u~ enters v~ (thread 0)
+        ok = mbar_wait(&bar[2], i & 1);
+        if (single && ok) wide_apply(sV, n_in, sLoc, sVal, dt);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicExch(&g_device_status, 1);
+            mbar_wait(&bar[2], i & 1);
+            break;
+        }
+        if (!single) {
+            for (int base = p0; base < p1; base += kThreads) {
+                __syncthreads();
+                int loc;
+                float val[2];
+                wide_fetch(a, base, p1, x0, z0, loc, val);
+                const int n = adj_compact<FWI_PSV>(loc, val, sLoc, sVal, sWarp);
+                __syncthreads();
+                wide_apply(sV, n, sLoc, sVal, dt);
+            }
+            __syncthreads();
+        }
+
+        // ---- v~' on the warp's interior rows, two columns per lane; t rows
+        // x-2 .. x+1 of t0 and t2 (the x-differentiated terms) in a register
+        // window, pre-masked (window index r <-> stress row ix0+1+r <-> grid
+        // row x0+ix0-2+r)
+        auto vel_interior = [&](auto zm) {
+            constexpr bool ZM = decltype(zm)::value;  // z masks needed (tile at a z edge)
+            float2 w0[RPW + 3], w2[RPW + 3];
+#pragma unroll
+            for (int r = 0; r < RPW + 3; r++) {
+                const int gr = x0 + ix0 - 2 + r;
+                const bool on = gr >= 1 && gr < nx - 2;
+                w0[r] = on ? ld2(sS + (ix0 + 1 + r) * SZ + col) : make_float2(0.f, 0.f);
+                w2[r] = on ? ld2(sS + 2 * FS + (ix0 + 1 + r) * SZ + col) : make_float2(0.f, 0.f);
+            }
+            // (D+z)^T of t at the two columns from the taps t[-2] .. t[2+1]
+            auto dzpT = [&](const float *t, float &d0, float &d1) {
+                const float2 A = ld2(t - 2), B = ld2(t), C = ld2(t + 2);
+                if constexpr (ZM) {
+                    d0 = cz1 * (A.y * pz[0][1] - B.x * pz[0][2]) - cz2 * (A.x * pz[0][0] - B.y * pz[0][3]);
+                    d1 = cz1 * (B.x * pz[1][1] - B.y * pz[1][2]) - cz2 * (A.y * pz[1][0] - C.x * pz[1][3]);
+                } else {
+                    d0 = cz1 * (A.y - B.x) - cz2 * (A.x - B.y);
+                    d1 = cz1 * (B.x - B.y) - cz2 * (A.y - C.x);
+                }
+            };
+#pragma unroll
+            for (int q = 0; q < RPW; q++) {
+                const int ix = ix0 + q, gx = x0 + ix;
+                const int vi = (ix + 1) * SZ + col;
+                if (!(zin0 && gx < nx)) {
+                    st2(sV + vi, 0.f, 0.f);
+                    st2(sV + FV + vi, 0.f, 0.f);
+                    continue;
+                }
+                const float *trow = sS + (ix + 3) * SZ + col;
+                const float dx0x = cx1 * (w0[q + 1].x - w0[q + 2].x) - cx2 * (w0[q].x - w0[q + 3].x);
+                const float dx0y = cx1 * (w0[q + 1].y - w0[q + 2].y) - cx2 * (w0[q].y - w0[q + 3].y);
+                const float dx2x = cx1 * (w2[q + 1].x - w2[q + 2].x) - cx2 * (w2[q].x - w2[q + 3].x);
+                const float dx2y = cx1 * (w2[q + 1].y - w2[q + 2].y) - cx2 * (w2[q].y - w2[q + 3].y);
+                float dz1x, dz1y, dz2x, dz2y;
+                dzpT(trow + FS, dz1x, dz1y);
+                dzpT(trow + 2 * FS, dz2x, dz2y);
+                // a_x = Dx+^T t0 + Dz+^T t2,  a_z = Dx+^T t2 + Dz+^T t1
+                const float2 buo = ld2(sP + vi), bnd = ld2(sP + FV + vi);
+                const float2 v0 = ld2(sV + vi), v1 = ld2(sV + FV + vi);
+                float vxx = bnd.x * (v0.x + (dx0x + dz2x)), vxy = bnd.y * (v0.y + (dx0y + dz2y));
+                float vzx = bnd.x * (v1.x + (dx2x + dz1x)), vzy = bnd.y * (v1.y + (dx2y + dz1y));
+                if (!zin1) vxy = vzy = 0.f;
+                const long long g = soff + (long long)gx * pitch + gz;
+                st2(a.vel_out[0] + g, vxx, vxy);
+                st2(a.vel_out[1] + g, vzx, vzy);
+                st2(sV + vi, buo.x * vxx, buo.y * vxy);
+                st2(sV + FV + vi, buo.x * vzx, buo.y * vzy);
+                float gbx = 0.f, gby = 0.f;
+                gbx += vxx * dsv[0][q].x;
+                gbx += vzx * dsv[1][q].x;
+                gby += vxy * dsv[0][q].y;
+                gby += vzy * dsv[1][q].y;
+                gk[2][q].x += gbx;
+                if (zin1) gk[2][q].y += gby;
+            }
+        };
+        if (zedge) vel_interior(std::true_type{});
+        else vel_interior(std::false_type{});
+        // the forward strain of the interior for the stress half: loads in
+        // flight during the halo and the barrier
+        float2 ef[3][RPW];
+#pragma unroll
+        for (int q = 0; q < RPW; q++) {
+            const int gx = x0 + ix0 + q;
+            const bool in = zin0 && gx < nx;
+            const long long g = soff + (long long)gx * pitch + gz;
+#pragma unroll
+            for (int k = 0; k < 3; k++) ef[k][q] = in ? ld2(a.ef[k] + g) : make_float2(0.f, 0.f);
+        }
+        // ---- v~' on the halo rows x0-1, x0+TX, x0+TX+1 and columns z0-1,
+        // z0+TZ, z0+TZ+1 (redundant with the neighbour tiles; masks per tap)
+        {
+            constexpr int HROW = 3 * RVZ, HC = HROW + 3 * TX;
+            auto mxp = [&](int k) -> float { return (k >= 1 && k < nx - 2) ? 1.f : 0.f; };
+            auto mzp = [&](int k) -> float { return (k >= 1 && k < nz - 2) ? 1.f : 0.f; };
+            for (int c = tid; c < HC; c += kThreads) {
+                int rx, rz;
+                if (c < HROW) {
+                    const int r3 = c / RVZ;
+                    rx = r3 == 0 ? 0 : TX + r3;
+                    rz = c - r3 * RVZ;
+                } else {
+                    const int c2 = c - HROW, k3 = c2 % 3;
+                    rx = 1 + c2 / 3;
+                    rz = k3 == 0 ? 0 : TZ + k3;
+                }
+                const int hx = x0 - 1 + rx, hz = z0 - 1 + rz;
+                const int vi = rx * SZ + rz + 3, si = (rx + 2) * SZ + rz + 3;
+                if (hx < 0 || hx >= nx || hz < 0 || hz >= nz) {
+                    sV[vi] = 0.f;
+                    sV[FV + vi] = 0.f;
+                    continue;
+                }
+                auto dxpT = [&](int f) -> float {
+                    const float *t = sS + f * FS + si;
+                    return cx1 * (t[-SZ] * mxp(hx - 1) - t[0] * mxp(hx)) -
+                           cx2 * (t[-2 * SZ] * mxp(hx - 2) - t[SZ] * mxp(hx + 1));
+                };
+                auto dzpT1 = [&](int f) -> float {
+                    const float *t = sS + f * FS + si;
+                    return cz1 * (t[-1] * mzp(hz - 1) - t[0] * mzp(hz)) - cz2 * (t[-2] * mzp(hz - 2) - t[1] * mzp(hz + 1));
+                };
+                const float acc0 = dxpT(0) + dzpT1(2), acc1 = dxpT(2) + dzpT1(1);
+                const float bnd = sP[FV + vi], b = sP[vi];
+                sV[vi] = b * (bnd * (sV[vi] + acc0));
+                sV[FV + vi] = b * (bnd * (sV[FV + vi] + acc1));
+            }
+        }
+        __syncthreads();
+        // t has been consumed: the next shot's sig~ streams in during the stress half
+        if (tid == 0 && shot + csize < nshots) issue_sig(shot + csize);
+        if (shot + csize < nshots) prefetch_entries(shot + csize);
+
+        // ---- sig~' and the stiffness gradient terms on the interior; b v~'
+        // rows x-1 .. x+2 in a register window, pre-masked (window index r
+        // <-> velocity row ix0+r <-> grid row x0+ix0-1+r)
+        auto stress_interior = [&](auto zm) {
+            constexpr bool ZM = decltype(zm)::value;
+            float2 w0[RPW + 3], w1[RPW + 3];
+#pragma unroll
+            for (int r = 0; r < RPW + 3; r++) {
+                const int gr = x0 + ix0 - 1 + r;
+                const bool on = gr >= 2 && gr < nx - 2;
+                w0[r] = on ? ld2(sV + (ix0 + r) * SZ + col) : make_float2(0.f, 0.f);
+                w1[r] = on ? ld2(sV + FV + (ix0 + r) * SZ + col) : make_float2(0.f, 0.f);
+            }
+            // (D-z)^T of b v~' at the two columns from the taps v[-1] .. v[2+1]
+            auto dzmT = [&](const float *v, float &d0, float &d1) {
+                const float2 A = ld2(v - 2), B = ld2(v), C = ld2(v + 2);
+                if constexpr (ZM) {
+                    d0 = cz1 * (B.x * mz[0][1] - B.y * mz[0][2]) - cz2 * (A.y * mz[0][0] - C.x * mz[0][3]);
+                    d1 = cz1 * (B.y * mz[1][1] - C.x * mz[1][2]) - cz2 * (B.x * mz[1][0] - C.y * mz[1][3]);
+                } else {
+                    d0 = cz1 * (B.x - B.y) - cz2 * (A.y - C.x);
+                    d1 = cz1 * (B.y - C.x) - cz2 * (B.x - C.y);
+                }
+            };
+#pragma unroll
+            for (int q = 0; q < RPW; q++) {
+                const int ix = ix0 + q, gx = x0 + ix;
+                if (!(zin0 && gx < nx)) continue;
+                const float *vrow = sV + (ix + 1) * SZ + col;
+                const float dx0x = cx1 * (w0[q + 1].x - w0[q + 2].x) - cx2 * (w0[q].x - w0[q + 3].x);
+                const float dx0y = cx1 * (w0[q + 1].y - w0[q + 2].y) - cx2 * (w0[q].y - w0[q + 3].y);
+                const float dx1x = cx1 * (w1[q + 1].x - w1[q + 2].x) - cx2 * (w1[q].x - w1[q + 3].x);
+                const float dx1y = cx1 * (w1[q + 1].y - w1[q + 2].y) - cx2 * (w1[q].y - w1[q + 3].y);
+                float dz0x, dz0y, dz1x, dz1y;
+                dzmT(vrow, dz0x, dz0y);
+                dzmT(vrow + FV, dz1x, dz1y);
+                const long long g = soff + (long long)gx * pitch + gz;
+                const float2 sxx = sg[0][q], szz = sg[1][q], sxz = sg[2][q];
+                float o0y = sxx.y + dx0y, o1y = szz.y + dz1y, o2y = sxz.y + (dz0y + dx1y);
+                if (!zin1) o0y = o1y = o2y = 0.f;
+                st2(a.sig_out[0] + g, sxx.x + dx0x, o0y);
+                st2(a.sig_out[1] + g, szz.x + dz1x, o1y);
+                st2(a.sig_out[2] + g, sxz.x + (dz0x + dx1x), o2y);
+                const float2 exx = ef[0][q], ezz = ef[1][q], exz = ef[2][q];
+                gk[0][q].x += dt * ((sxx.x + szz.x) * (exx.x + ezz.x));
+                gk[1][q].x += dt * (2.f * (sxx.x * exx.x + szz.x * ezz.x) + sxz.x * exz.x);
+                if (zin1) {
+                    gk[0][q].y += dt * ((sxx.y + szz.y) * (exx.y + ezz.y));
+                    gk[1][q].y += dt * (2.f * (sxx.y * exx.y + szz.y * ezz.y) + sxz.y * exz.y);
+                }
+            }
+        };
+        if (zedge) stress_interior(std::true_type{});
+        else stress_interior(std::false_type{});
+        __syncthreads();
+        // the v~ buffer is free: the next shot streams into it
+        if (tid == 0 && shot + csize < nshots) issue_vel(shot + csize);
+    }
+    if (crank >= nshots) mbar_wait(&bar[0], 0);  // no shot: let the model copies land
+
+    // ---- cluster sum of the gradient terms, in rank order, into FP64
+    float *part = smem;
+#pragma unroll
+    for (int k = 0; k < T::NK; k++)
+#pragma unroll
+        for (int q = 0; q < RPW; q++) st2(part + k * TX * TZ + (ix0 + q) * TZ + 2 * lane, gk[k][q].x, gk[k][q].y);
+    cluster.sync();
+    // four cells per thread and pass: their FP64 gradient loads in flight together
+    const int chunk = (TX * TZ + csize - 1) / csize, c0 = crank * chunk;
+    for (int e0 = tid; e0 < T::NK * chunk; e0 += 4 * kThreads) {
+        double kv[4];
+        long long gi[4];
+        int kk[4], ci[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int e = e0 + u * kThreads;
+            kk[u] = -1;
+            if (e < T::NK * chunk) {
+                const int k = e / chunk, c = c0 + (e - k * chunk);
+                const int gx = x0 + c / TZ, gzc = z0 + c % TZ;
+                if (c < TX * TZ && a.k[k] && gx < nx && gzc < nz) {
+                    kk[u] = k;
+                    ci[u] = k * TX * TZ + c;
+                    gi[u] = (long long)gx * pitch + gzc;
+                }
+            }
+            kv[u] = kk[u] >= 0 ? a.k[kk[u]][gi[u]] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            if (kk[u] < 0) continue;
+            double s = 0.0;
+            for (int j = 0; j < csize; j++) s += (double)cluster.map_shared_rank(part, j)[ci[u]];
+            a.k[kk[u]][gi[u]] = kv[u] + s;
+        }
+    }
+    cluster.sync();  // keep this CTA's shared memory alive until every rank has read it
+}
+
+static int wide_maps(const fwi_batch *b, WideMaps &m) {
+    using T = WideTile;
+    const int cur = b->cur, nx = b->nx, pitch = b->pitch, ns = b->nshots;
+    int rc = 0;
+    for (int f = 0; f < 3 && !rc; f++) rc = encode_map(&m.sig[f], b->sig[cur][f], 3, pitch, nx, ns, T::SZ, T::SX);
+    for (int q = 0; q < 2 && !rc; q++) rc = encode_map(&m.vel[q], b->vel[cur][q], 3, pitch, nx, ns, T::SZ, T::VX);
+    const float *lm[2] = {b->lam, b->mu};
+    for (int f = 0; f < 2 && !rc; f++) rc = encode_map(&m.lm[f], lm[f], 2, pitch, nx, 1, T::SZ, T::SX);
+    const float *vp[2] = {b->buo, b->bound};
+    for (int p = 0; p < 2 && !rc; p++) rc = encode_map(&m.vp[p], vp[p], 2, pitch, nx, 1, T::SZ, T::VX);
+    return rc;
+}
+
 // Tensor maps of one transposed step.
 template <int MODE>
 static int adjoint_maps(const fwi_batch *b, const AdjArgs &a, AdjMaps &m) {
@@ -1626,6 +2082,37 @@ static int launch_adjoint(const fwi_batch *b, const AdjArgs &a, cudaStream_t st)
     return check_launch("adjoint_kernel");
 }
 
+static int launch_adjoint_wide(const fwi_batch *b, const AdjArgs &a, cudaStream_t st) {
+    using T = WideTile;
+    static bool set = false;
+    if (!set) {
+        cudaError_t e = cudaFuncSetAttribute(adjoint_wide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)T::bytes);
+        if (e != cudaSuccess) return set_error(FWI_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+        set = true;
+    }
+    WideMaps m;
+    int rc = wide_maps(b, m);
+    if (rc) return rc;
+    const int tz = (b->nz + T::TZ - 1) / T::TZ, tx = (b->nx + T::TX - 1) / T::TX;
+    const int C = adjoint_cluster(b->nshots, (long long)tz * tx, 2);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(tz, tx, C);
+    cfg.blockDim = dim3(kThreads, 1, 1);
+    cfg.dynamicSmemBytes = T::bytes;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 1;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = C;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, adjoint_wide_kernel, a, m);
+    if (e != cudaSuccess) return set_error(FWI_ECUDA, "adjoint_wide_kernel launch: %s", cudaGetErrorString(e));
+    return check_launch("adjoint_wide_kernel");
+}
+
 // One transposed step (forward step `it`, adjoint state it+1 -> it) with
 // its gradient terms.
 int launch_adjoint_step(const fwi_batch *b, int it, cudaStream_t st) {
@@ -1675,7 +2162,7 @@ int launch_adjoint_step(const fwi_batch *b, int it, cudaStream_t st) {
     a.g[1] = mode == FWI_SH ? nullptr : b->stf[2];
     switch (mode) {
         case FWI_SH: return launch_adjoint<FWI_SH>(b, a, st);
-        case FWI_PSV: return launch_adjoint<FWI_PSV>(b, a, st);
+        case FWI_PSV: return b->adj_tile == 1 ? launch_adjoint<FWI_PSV>(b, a, st) : launch_adjoint_wide(b, a, st);
         default: return launch_adjoint<FWI_SPIN>(b, a, st);
     }
 }

@@ -392,3 +392,56 @@ def test_two_level_checkpointing_is_bit_identical(mode):
     # the illumination is sampled at the multiples of the segment whether or not a stored tail
     # takes the last steps, so it does not depend on the memory the tail got
     assert torch.equal(il1, out[2][2]) and float(il1.max()) > 0
+
+
+@pytest.mark.parametrize("nx,nz,nshots,nrec", [(70, 133, 5, 300), (96, 128, 3, 40), (33, 37, 1, 7), (64, 200, 9, 12)])
+def test_psv_wide_tile_transposed_step_is_bit_identical(nx, nz, nshots, nrec):
+    """The P-SV transposed step on 32 x 64 tiles (two z columns per thread,
+    the default) against 32 x 32 tiles (one column per thread), from the
+    same random adjoint state, segment stores and receiver injections: the
+    adjoint fields agree bit for bit, the FP64 gradient terms to the
+    rounding of their summation over a cluster's shots (the two tilings pick
+    different cluster sizes).  Grids that are not multiples of the tiles, an
+    odd nz, one shot, and more injection entries per shot than one CTA's
+    list holds (300)."""
+    from seispie_b200.engine import Grid, ShotBatch, adjoint_injection_lists, build_model
+    rng = np.random.default_rng(nx * 1000 + nz)
+    h, dt, nt, it = 10.0, 1e-3, 6, 3
+    grid = Grid(nx, nz, h, h)
+    npt = nx * nz
+    prm = dict(rho=2600 * (1 + 0.05 * rng.random(npt)), lam=8.1e9 * (1 + 0.05 * rng.random(npt)),
+               mu=8.1e9 * (1 + 0.05 * rng.random(npt)))
+    m = build_model("psv", grid, dt, prm, (8, 0.05, 1, 1, 1, 0), "cuda")
+    rec = rng.integers(0, npt, nrec).astype(np.int32)
+    shape = (nshots, nx, grid.pitch)
+
+    def field():
+        t = torch.randn(shape, device="cuda")
+        t[..., nz:] = 0.0  # padding cells stay zero
+        return t
+
+    state = [field() for _ in range(5)]
+    seg_e = [field()[None] for _ in range(3)] + [None] * 3
+    seg_ds = [field()[None], None, field()[None]]
+    stf = [torch.randn(nshots * nrec * nt, device="cuda"), None, torch.randn(nshots * nrec * nt, device="cuda")]
+    inj = adjoint_injection_lists(nshots, rec)
+    out = []
+    for tile in (0, 1):
+        b = ShotBatch(m, nshots, nt, rec)
+        b.adj_tile = tile
+        for t, s in zip(b.sig[0] + b.vel[0], state):
+            t.copy_(s)
+        k = [torch.zeros((nx, grid.pitch), dtype=torch.float64, device="cuda") for _ in range(3)]
+        d = b.desc(inj=inj, stf=stf, record=False, kernels=k)
+        b.set_segment(d, seg_e, seg_ds, it, 1)
+        b.run_transposed(d, it + 1, 1)
+        torch.cuda.synchronize()
+        assert d.cur == 1
+        out.append(([t.clone() for t in b.sig[1] + b.vel[1]], k))
+    (f0, k0), (f1, k1) = out
+    for a, c in zip(f0, f1):
+        assert float(a.abs().max()) > 0
+        assert torch.equal(a, c)
+    for a, c in zip(k0, k1):
+        scale = float(c.abs().max())
+        assert scale > 0 and float((a - c).abs().max()) <= 1e-6 * scale
