@@ -120,8 +120,12 @@ def cmd_gen(a):
         amp = float(rng.uniform(0.03, 0.08))
         path = os.path.abspath(os.path.join(a.out, "pairs_%04d.npz" % c))
         with tempfile.TemporaryDirectory() as root:
-            _, _, mu_true = run_inversion(root, a.nx, a.nz, a.shots, a.nt, a.niter, board, amp, "lbfgs_learned",
-                                          "record_pairs = %s\n" % path, perturb=a.perturb)
+            try:
+                _, _, mu_true = run_inversion(root, a.nx, a.nz, a.shots, a.nt, a.niter, board, amp,
+                                              "lbfgs_learned", "record_pairs = %s\n" % path, perturb=a.perturb)
+            except RuntimeError as e:  # the reference's line search gives up on a non-convex fit: skip the case
+                print(json.dumps({"case": c, "skipped": str(e)}), flush=True)
+                continue
         if os.path.exists(path):
             z = dict(np.load(path))
             z["m_true"] = np.asarray(mu_true, np.float32).ravel()  # for the model-error target
