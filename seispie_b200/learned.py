@@ -41,6 +41,8 @@ from .unet import UNet
 WEIGHTS_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights")
 DEFAULT_WEIGHTS = os.path.join(WEIGHTS_DIR, "unet_psv_mu.npz")
 ERROR_WEIGHTS = os.path.join(WEIGHTS_DIR, "unet_psv_mu_error.npz")
+# the model-error target trained on about 860 pairs of 512 x 256, 32-shot, nt 2500 mu inversions
+ERROR_WEIGHTS_512 = os.path.join(WEIGHTS_DIR, "unet_psv_mu_error_512.npz")
 
 
 def _pad8(n: int) -> int:
