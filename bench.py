@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--autotune", action="store_true", help="time every tile variant and report the best")
     ap.add_argument("--overlap", type=int, default=1, choices=[0, 1],
                     help="1: recompute segment s-1 on a second stream while segment s is transposed")
+    ap.add_argument("--density", type=int, default=0, choices=[0, 1],
+                    help="1: also the density kernel (stores the divergence per step); 0: lambda and mu kernels")
     ap.add_argument("--overlap-ctas", type=int, default=0,
                     help="with --overlap: resident CTAs per SM of the recomputing step (0: all that fit)")
     ap.add_argument("--shard", action="store_true",
@@ -342,11 +344,14 @@ def main():
         # per-step stores of the last steps kept from the forward sweep: the longest tail that fits
         # 90 % of the free HBM with the checkpoints, segment stores, wavefields and traces
         free, _ = torch.cuda.mem_get_info(dev)
-        tail = max_tail_bytes(nt, FWI_PSV, nshots, m_init.grid, 0.9 * free, a.nrec, overlap=bool(a.overlap))
+        # the mu kernel (the reference's) and the lambda kernel, no density kernel: no divergence stores
+        tail = max_tail_bytes(nt, FWI_PSV, nshots, m_init.grid, 0.9 * free, a.nrec, overlap=bool(a.overlap),
+                              density=bool(a.density))
         ea = ExactAdjoint(m_init, nt, sid, lambda s: mine[s], nshots, stf, rid, tile=a.tile, tail_memory=tail,
-                          overlap=bool(a.overlap), overlap_ctas=a.overlap_ctas)
+                          overlap=bool(a.overlap), overlap_ctas=a.overlap_ctas, density=bool(a.density))
         checkpointing = {"segment": ea.K, "checkpoints": ea.nseg, "stored_tail_steps": ea.tail,
                          "overlap": ea.overlap, "overlap_ctas": ea.overlap_ctas}
+        kernels = ["lam", "mu"] + (["rho"] if ea.density else [])
         grads = [torch.empty((nshots, a.nrec, nt), dtype=torch.float32, device=dev) if c != 1 else None
                  for c in range(3)]
         b = ea.fwd
@@ -496,6 +501,7 @@ def main():
         extra = {"tile": _lib.tile_label(b_tile(a, tuned)), "misfit": misfit_total}
         if a.gradient == "exact":
             extra["checkpointing"] = checkpointing
+            extra["kernels"] = kernels
             extra["tile"] = "row-marching (displacement-free)"
         if tuned:
             extra["autotune_ms_per_fwd_step"] = tuned[2]
@@ -532,7 +538,7 @@ def run_e2e(a, w, dev, world, rank, data, ntot):
     s.config = dict(nt=str(a.nt), dt=str(w["dt"]), sh="no", psv="yes", spin="no", abs_left="yes", abs_right="yes",
                     abs_top="no", abs_bottom="yes", abs_width="20", abs_alpha="0.015", save_coordinates="",
                     combine_sources="no", save_snapshot="0", adjoint_interval=str(a.sae), smooth=str(a.sigma),
-                    tile=str(a.tile))
+                    tile=str(a.tile), kernel_rho="yes" if a.density else "no")
     s.path = dict(model_init=td + "/init", model_true=td + "/init", sources=td + "/src.dat",
                   stations=td + "/rec.dat", output=td + "/out")
     if world > 1:

@@ -39,12 +39,19 @@ def state_fields(mode: int, grid: Grid) -> int:
     return NS[mode] + (1 if engine.displacement_free_ok(mode, grid) else 2) * NV[mode]
 
 
-def default_segment(nt: int, mode: int, nshots: int, grid: Grid, budget_bytes: float | None = None) -> int:
+def step_fields(mode: int, density: bool = True) -> int:
+    """Fields stored per step for the transposed step: the stress-update
+    terms, plus the divergences where the density terms are wanted."""
+    return strain_fields(mode) + (NV[mode] if density else 0)
+
+
+def default_segment(nt: int, mode: int, nshots: int, grid: Grid, budget_bytes: float | None = None,
+                    density: bool = True) -> int:
     """Segment length K minimising checkpoint + segment memory
     (nt/K * S fields + K * (NE+NV) fields, S = state_fields), then shrunk to
     the budget."""
     state = state_fields(mode, grid)
-    per_step = strain_fields(mode) + NV[mode]
+    per_step = step_fields(mode, density)
     k = max(1, int(round(math.sqrt(nt * state / per_step))))
     if budget_bytes:
         field = 4 * nshots * grid.nx * grid.pitch
@@ -54,17 +61,17 @@ def default_segment(nt: int, mode: int, nshots: int, grid: Grid, budget_bytes: f
 
 
 def fixed_bytes(nt: int, mode: int, nshots: int, grid: Grid, nrec: int = 0, segment: int | None = None,
-                overlap: bool = False) -> int:
+                overlap: bool = False, density: bool = True) -> int:
     """Upper bound of the device bytes an ExactAdjoint (levels = 1) holds
     besides its stored tail: checkpoints every K steps over all nt steps, one
     segment of per-step stores (two with overlap), the wavefields of the
     forward and adjoint batches (ping-pong stress and velocity, displacement
     where kept) and, per velocity component, the traces, the observed data
     and the trace gradients.  A stored tail has to fit in what is left."""
-    k = segment or default_segment(nt, mode, nshots, grid)
+    k = segment or default_segment(nt, mode, nshots, grid, density=density)
     field = 4 * nshots * grid.nx * grid.pitch
     state = state_fields(mode, grid)
-    per_step = strain_fields(mode) + NV[mode]
+    per_step = step_fields(mode, density)
     batch = 2 * NS[mode] + 2 * NV[mode] + (state - NS[mode] - NV[mode])
     segs = 2 if overlap else 1
     return ((math.ceil(nt / k) * state + segs * k * per_step + 2 * batch) * field
@@ -72,17 +79,17 @@ def fixed_bytes(nt: int, mode: int, nshots: int, grid: Grid, nrec: int = 0, segm
 
 
 def max_tail_bytes(nt: int, mode: int, nshots: int, grid: Grid, budget_bytes: float, nrec: int = 0,
-                   segment: int | None = None, overlap: bool = False) -> int:
+                   segment: int | None = None, overlap: bool = False, density: bool = True) -> int:
     """Largest stored tail (as ExactAdjoint's tail_memory, in bytes) whose
     ExactAdjoint (levels = 1) fits budget_bytes in all: checkpoints of the
     steps before the tail, one segment of per-step stores (two with
     overlap), the tail's per-step stores, both batches' wavefields and the
     trace arrays (the terms of fixed_bytes).  A longer tail needs fewer
     checkpoints."""
-    k = segment or default_segment(nt, mode, nshots, grid)
+    k = segment or default_segment(nt, mode, nshots, grid, density=density)
     field = 4 * nshots * grid.nx * grid.pitch
     state = state_fields(mode, grid)
-    per_step = strain_fields(mode) + NV[mode]
+    per_step = step_fields(mode, density)
     batch = 2 * NS[mode] + 2 * NV[mode] + (state - NS[mode] - NV[mode])
     traces = 3 * 4 * nshots * nrec * nt * NV[mode]
     segs = 2 if overlap else 1
@@ -136,11 +143,16 @@ class ExactAdjoint:
     segment s run, so that the two kernels share the SMs (same values, so
     the same gradient bit for bit); overlap_ctas caps the resident CTAs per
     SM of the recomputing row-marching step (0: no cap), leaving room for
-    the transposed step's CTAs."""
+    the transposed step's CTAs.
+
+    density = False: no density terms (backward returns None for dL/dbuo,
+    and for spin dL/dbuo_j), so no divergence is stored per step: a P-SV
+    step stores 3 fields instead of 5, the stored tail holds 5/3 as many
+    steps, and the lambda / mu terms are the same bit for bit."""
 
     def __init__(self, model: DeviceModel, nt: int, src_id, isrc_of_shot, nshots: int, stf, rec_id,
                  segment: int | None = None, tile: int = 0, levels: int = 1, sub_segment: int | None = None,
-                 tail_memory: float = 0.0, overlap: bool = False, overlap_ctas: int = 0):
+                 tail_memory: float = 0.0, overlap: bool = False, overlap_ctas: int = 0, density: bool = True):
         self.model, self.nt, self.nshots = model, int(nt), int(nshots)
         self.rec_id = np.asarray(rec_id, np.int32)
         self.mode = model.mode
@@ -151,14 +163,15 @@ class ExactAdjoint:
             raise ValueError("overlap needs levels = 1")
         self.levels = levels
         if levels == 1:
-            self.K = segment or default_segment(self.nt, self.mode, self.nshots, g)
+            self.K = segment or default_segment(self.nt, self.mode, self.nshots, g, density=density)
             self.K2 = self.K
         else:
             k1, k2 = two_level_segments(self.nt, self.mode)
             self.K = segment or k1
             self.K2 = min(sub_segment or k2, self.K)
         field = 4 * self.nshots * g.nx * g.pitch
-        per_step = (strain_fields(self.mode) + NV[self.mode]) * field
+        self.density = bool(density)
+        per_step = step_fields(self.mode, self.density) * field
         self.tail = min(self.nt, int(max(0.0, tail_memory) // per_step))
         self.t0 = self.nt - self.tail  # steps [t0, nt) keep their stores from the forward sweep
         self.nseg = math.ceil(self.t0 / self.K)
@@ -180,7 +193,7 @@ class ExactAdjoint:
         self.seg_ds = [None, None, None]
         for k in range(strain_fields(self.mode)):
             self.seg_e[k] = torch.empty((self.K2,) + shape, dtype=torch.float32, device=dev)
-        for c in COMP[self.mode][: NV[self.mode]]:
+        for c in COMP[self.mode][: NV[self.mode]] if self.density else ():
             self.seg_ds[c] = torch.empty((self.K2,) + shape, dtype=torch.float32, device=dev)
         self.overlap = bool(overlap) and self.nseg > 1
         self.overlap_ctas = int(overlap_ctas)
@@ -192,7 +205,7 @@ class ExactAdjoint:
         if self.tail:
             for k in range(strain_fields(self.mode)):
                 self.tail_e[k] = torch.empty((self.tail,) + shape, dtype=torch.float32, device=dev)
-            for c in COMP[self.mode][: NV[self.mode]]:
+            for c in COMP[self.mode][: NV[self.mode]] if self.density else ():
                 self.tail_ds[c] = torch.empty((self.tail,) + shape, dtype=torch.float32, device=dev)
 
     def forward(self) -> list:
@@ -238,13 +251,17 @@ class ExactAdjoint:
         [nshots, nrec, nt] in forward time order).  Returns FP64
         (dL/dlam, dL/dmu, dL/dbuo) on [nx, pitch] (dL/dlam is zero for SH);
         spin adds (dL/dnu, dL/dmnc, dL/dbuo_j) with mnc = mu_c + nu_c and
-        buo_j = dt/j.  Spin losses may depend on ux and uz only."""
+        buo_j = dt/j.  Spin losses may depend on ux and uz only.  Without
+        density terms (density = False) dL/dbuo and dL/dbuo_j are None."""
         if self.mode == FWI_SPIN and g_traces[1] is not None:
             raise ValueError("the spin adjoint injects x and z trace gradients only (no uy_c term)")
         gr = self.model.grid
         dev = self.model.device
         k = [torch.zeros((gr.nx, gr.pitch), dtype=torch.float64, device=dev)
              for _ in range(6 if self.mode == FWI_SPIN else 3)]
+        if not self.density:  # the buoyancy slots: dL/dbuo (2) and, for spin, dL/dbuo_j (5)
+            for q in ((2, 5) if self.mode == FWI_SPIN else (2,)):
+                k[q] = None
         stf = [None, None, None]
         for c in range(3):
             if g_traces[c] is not None and self.fwd.obs[c] is not None:
@@ -373,8 +390,9 @@ class Seismograms(torch.autograd.Function):
         engine.check(lib.fwi_set_bound(engine.ptr(m.bound), g.nx, g.nz, g.pitch, int(w), float(a), int(l), int(r),
                                        int(b), int(t), engine.stream_handle(None)), "fwi_set_bound")
         m.prepare()
+        # the divergence stores only where rho needs a gradient
         ea = ExactAdjoint(m, setup.nt, setup.src_id, setup.isrc_of_shot, setup.nshots, setup.stf, setup.rec_id,
-                          segment=setup.segment)
+                          segment=setup.segment, density=bool(ctx.needs_input_grad[2]))
         tr = ea.forward()
         comps = [c for c in range(3) if tr[c] is not None]
         ctx.ea, ctx.comps, ctx.setup = ea, comps, setup
@@ -394,9 +412,9 @@ class Seismograms(torch.autograd.Function):
         dlam = k_lam[:, :nz].reshape(g.nx, nz)
         dmu = k_mu[:, :nz].reshape(g.nx, nz)
         # buo = dt/rho rounded to float32 -> dL/drho = -dL/dbuo * dt / rho^2
-        drho = -k_buo[:, :nz].reshape(g.nx, nz) * ctx.setup.dt / rho.double() ** 2
+        drho = None if k_buo is None else (-k_buo[:, :nz].reshape(g.nx, nz) * ctx.setup.dt / rho.double() ** 2).float()
         ctx.ea = None
-        return dlam.float(), dmu.float(), drho.float(), None
+        return dlam.float(), dmu.float(), drho, None
 
 
 class AcquisitionSetup:

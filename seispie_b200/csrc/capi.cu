@@ -301,9 +301,13 @@ int fwi_run_transposed(fwi_batch *b, int it_hi, int nsteps, void *stream) {
             b->seg0 + b->nseg);
     const int cx = b->mode == FWI_SH ? 1 : 0;
     const int ne = b->mode == FWI_SH ? 2 : b->mode == FWI_PSV ? 3 : 6;
-    bool stores = b->seg_ds[cx] && (b->mode == FWI_SH || b->seg_ds[2]) && (b->mode != FWI_SPIN || b->seg_ds[1]);
+    // the divergence stores feed only the density terms (k_rho, spin also k_buoj)
+    const bool ds = b->seg_ds[cx] && (b->mode == FWI_SH || b->seg_ds[2]) && (b->mode != FWI_SPIN || b->seg_ds[1]);
+    bool stores = true;
     for (int k = 0; k < ne; k++) stores = stores && b->seg_e[k];
-    REQUIRE(stores, "fwi_run_transposed: the segment stores seg_e / seg_ds are required");
+    REQUIRE(stores, "fwi_run_transposed: the segment stores seg_e are required");
+    REQUIRE(ds || (!b->k_rho && !(b->mode == FWI_SPIN && b->k_buoj)),
+            "fwi_run_transposed: the density kernels need the divergence stores seg_ds");
     REQUIRE(b->k_mu, "fwi_run_transposed: k_mu is required");
     REQUIRE(b->adj_tile == 0 || b->adj_tile == 1, "fwi_run_transposed: adj_tile must be 0 or 1 (got %d)", b->adj_tile);
     if (b->inj_ptr) {

@@ -1061,7 +1061,7 @@ struct AdjArgs {
     float cx1, cx2, cz1, cz2, dt, dt2;
     float *sig_out[6];
     float *vel_out[3];
-    const float *dsf[3];  // forward divergence of step it, per velocity component
+    const float *dsf[3];  // forward divergence of step it, per velocity component (NULL: no density terms)
     const float *ef[6];   // forward stress-update terms of v(it+1) (fwi_batch.seg_e)
     double *k[6];         // SH: dL/dmu, dL/dbuo | P-SV: dL/dlam, dL/dmu, dL/dbuo |
                           // spin: dL/dlam, dL/dmu, dL/dnu, dL/dmnc, dL/dbuo, dL/dbuo_j ([nx][pitch], NULL skips)
@@ -1288,7 +1288,7 @@ __global__ void __launch_bounds__(kThreads, MODE == FWI_SH ? 4 : MODE == FWI_PSV
             const int gx = x0 + ix0 + q;
             const bool in = zin && gx < nx;
 #pragma unroll
-            for (int c = 0; c < NV; c++) dsv[c][q] = in ? a.dsf[c][soff + (long long)gx * pitch + gz] : 0.f;
+            for (int c = 0; c < NV; c++) dsv[c][q] = (in && a.dsf[0]) ? a.dsf[c][soff + (long long)gx * pitch + gz] : 0.f;
         }
         const int p0 = a.inj_ptr ? a.inj_ptr[shot] : 0, p1 = a.inj_ptr ? a.inj_ptr[shot + 1] : 0;
         const bool single = p1 - p0 <= kThreads;
@@ -1722,7 +1722,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             const bool in = zin0 && gx < nx;
             const long long g = soff + (long long)gx * pitch + gz;
 #pragma unroll
-            for (int c = 0; c < 2; c++) dsv[c][q] = in ? ld2(a.dsf[c] + g) : make_float2(0.f, 0.f);
+            for (int c = 0; c < 2; c++) dsv[c][q] = (in && a.dsf[0]) ? ld2(a.dsf[c] + g) : make_float2(0.f, 0.f);
         }
         const bool single = p1 - p0 <= kThreads;
         int n_in = 0;
@@ -2138,7 +2138,10 @@ int launch_adjoint_step(const fwi_batch *b, int it, cudaStream_t st) {
     const long long field = (long long)b->nshots * b->nx * b->pitch;
     const long long slot = it - b->seg0;
     for (int k = 0; k < 6; k++) a.ef[k] = k < ne ? b->seg_e[k] + slot * field : nullptr;
-    for (int q = 0; q < 3; q++) a.dsf[q] = q < nv ? b->seg_ds[comp_slot(mode, q)] + slot * field : nullptr;
+    // divergence stores (all components or none: without them the density terms are skipped)
+    bool ds = true;
+    for (int q = 0; q < nv; q++) ds = ds && b->seg_ds[comp_slot(mode, q)];
+    for (int q = 0; q < 3; q++) a.dsf[q] = (ds && q < nv) ? b->seg_ds[comp_slot(mode, q)] + slot * field : nullptr;
     for (int k = 0; k < 6; k++) a.k[k] = nullptr;
     if (mode == FWI_SH) {
         a.k[0] = b->k_mu;

@@ -239,11 +239,18 @@ class b200:
         if snapshots and self._exact(mode):
             from ..adjoint import fixed_bytes
             # checkpoints, segment stores, both batches' wavefields, traces, data and trace gradients
-            return fixed_bytes(self.nt, mode, 1, g, self.nrec, overlap=True)
+            return fixed_bytes(self.nt, mode, 1, g, self.nrec, overlap=True, density=self._density(mode))
         b = (2 * ns + 3 * nv) * field + 4 * self.nrec * self.nt * nv * 3
         if snapshots:
             b += self.nsa * min(nv, 2) * field * (2 if (mode != FWI_SH and self.kernel_rho) else 1)
         return b
+
+    def _density(self, mode) -> bool:
+        """Exact gradient with the density kernel?  Spin always (its dt/j
+        kernel shares the stores); SH and P-SV with kernel_rho = yes: without
+        it the forward stores no divergence per step (3 instead of 5 fields
+        for P-SV), which lengthens the stored tail."""
+        return mode == FWI_SPIN or self.kernel_rho
 
     def _exact(self, mode) -> bool:
         """Gradient by the exact discrete adjoint?  Default: yes for P-SV and
@@ -275,11 +282,12 @@ class b200:
                 tail = 0.0
                 if self.batch_memory <= 0:
                     tail = max_tail_bytes(nt, mode, n, self.model.grid, 0.85 * self._free_bytes(), nrec,
-                                          overlap=True)
+                                          overlap=True, density=self._density(mode))
                 # two segments of per-step stores: the next segment is recomputed on a second stream
                 # while this one is transposed
                 ea = ExactAdjoint(self.model, nt, self.src_id, lambda s: -1 if combine else chunk[s], n,
-                                  self._stf(mode), self.rec_id, tile=self.tile, tail_memory=tail, overlap=True)
+                                  self._stf(mode), self.rec_id, tile=self.tile, tail_memory=tail, overlap=True,
+                                  density=self._density(mode))
                 # the observed traces are stacked into pinned host memory on worker threads while
                 # this thread enqueues the forward sweep, then uploaded on a copy stream that the
                 # misfit waits for
@@ -304,9 +312,10 @@ class b200:
         k_lam, k_mu, k_buo = ks[:3]
         self.k_lam_f64 += self.dt * k_lam
         self.k_mu_f64 += self.dt * k_mu
-        # buo = dt/rho: dchi/drho = -dchi/dbuo * dt / rho^2
-        rho = self.model.rho.double()
-        self.k_rho_f64 -= self.dt * k_buo * self.dt / torch.where(rho > 0, rho * rho, torch.ones_like(rho))
+        if k_buo is not None:
+            # buo = dt/rho: dchi/drho = -dchi/dbuo * dt / rho^2
+            rho = self.model.rho.double()
+            self.k_rho_f64 -= self.dt * k_buo * self.dt / torch.where(rho > 0, rho * rho, torch.ones_like(rho))
         if mode == FWI_SPIN:
             # spin: nu, mu_c and nu_c (both through mnc = mu_c + nu_c), j through dt/j
             k_nu, k_mnc, k_buoj = ks[3:]
@@ -449,7 +458,7 @@ class b200:
         """Forward of one shot set with the exact adjoint's checkpoints kept."""
         from ..adjoint import ExactAdjoint
         ea = ExactAdjoint(self.model, self.nt, self.src_id, lambda s: isrc, 1, self._stf(mode), self.rec_id,
-                          tile=self.tile)
+                          tile=self.tile, density=self._density(mode))
         tr = ea.forward()
         self.illum_f64 += ea.illum
         self._adjoint_state[mode] = ("exact", ea)

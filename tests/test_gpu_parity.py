@@ -410,9 +410,14 @@ def test_psv_run_adjoint_per_shot_equals_batched_gradient(tmp_path):
     reference's P-SV adjoint cannot run) gives the batched exact gradient of
     run_kernel: k_lam, k_mu, k_rho and the misfit."""
     g = load_golden("sh_grad")
-    s = _plugin_case(tmp_path, g, sh="no", psv="yes")
+    s = _plugin_case(tmp_path / "a", g, sh="no", psv="yes", kernel_rho="yes")
     misfit_b = s.run_kernel(1)[0]
     batched = [k.clone() for k in (s.k_lam_f64, s.k_mu_f64, s.k_rho_f64)]
+    # without kernel_rho no divergence is stored: the same lambda / mu kernels bit for bit, no rho kernel
+    s2 = _plugin_case(tmp_path / "b", g, sh="no", psv="yes")
+    assert s2.run_kernel(1)[0] == misfit_b
+    assert torch.equal(s2.k_lam_f64, batched[0]) and torch.equal(s2.k_mu_f64, batched[1])
+    assert float(s2.k_rho_f64.abs().max()) == 0
     s.setup_adjoint()
     s.clear_kernels()
     misfit = 0.0
