@@ -46,12 +46,12 @@ def step_fields(mode: int, density: bool = True) -> int:
 
 
 def default_segment(nt: int, mode: int, nshots: int, grid: Grid, budget_bytes: float | None = None,
-                    density: bool = True) -> int:
+                    density: bool = True, overlap: bool = False) -> int:
     """Segment length K minimising checkpoint + segment memory
-    (nt/K * S fields + K * (NE+NV) fields, S = state_fields), then shrunk to
-    the budget."""
+    (nt/K * S fields + B * K * P fields: S = state_fields, P = step_fields,
+    B = 1 segment buffer, 2 with overlap), then shrunk to the budget."""
     state = state_fields(mode, grid)
-    per_step = step_fields(mode, density)
+    per_step = step_fields(mode, density) * (2 if overlap else 1)
     k = max(1, int(round(math.sqrt(nt * state / per_step))))
     if budget_bytes:
         field = 4 * nshots * grid.nx * grid.pitch
@@ -68,7 +68,7 @@ def fixed_bytes(nt: int, mode: int, nshots: int, grid: Grid, nrec: int = 0, segm
     forward and adjoint batches (ping-pong stress and velocity, displacement
     where kept) and, per velocity component, the traces, the observed data
     and the trace gradients.  A stored tail has to fit in what is left."""
-    k = segment or default_segment(nt, mode, nshots, grid, density=density)
+    k = segment or default_segment(nt, mode, nshots, grid, density=density, overlap=overlap)
     field = 4 * nshots * grid.nx * grid.pitch
     state = state_fields(mode, grid)
     per_step = step_fields(mode, density)
@@ -86,7 +86,7 @@ def max_tail_bytes(nt: int, mode: int, nshots: int, grid: Grid, budget_bytes: fl
     overlap), the tail's per-step stores, both batches' wavefields and the
     trace arrays (the terms of fixed_bytes).  A longer tail needs fewer
     checkpoints."""
-    k = segment or default_segment(nt, mode, nshots, grid, density=density)
+    k = segment or default_segment(nt, mode, nshots, grid, density=density, overlap=overlap)
     field = 4 * nshots * grid.nx * grid.pitch
     state = state_fields(mode, grid)
     per_step = step_fields(mode, density)
@@ -163,7 +163,7 @@ class ExactAdjoint:
             raise ValueError("overlap needs levels = 1")
         self.levels = levels
         if levels == 1:
-            self.K = segment or default_segment(self.nt, self.mode, self.nshots, g, density=density)
+            self.K = segment or default_segment(self.nt, self.mode, self.nshots, g, density=density, overlap=overlap)
             self.K2 = self.K
         else:
             k1, k2 = two_level_segments(self.nt, self.mode)

@@ -130,8 +130,14 @@ def test_exact_adjoint_fixed_bytes():
     # and 2 components x (traces, data, trace gradients)
     want = (78 * 5 + 77 * 5 + 2 * 10) * field + 3 * 4 * 64 * 256 * 6000 * 2
     assert fixed_bytes(6000, FWI_PSV, 64, g, 256) == want
-    # the overlapped backward holds a second segment of stores
-    assert fixed_bytes(6000, FWI_PSV, 64, g, 256, overlap=True) == want + 77 * 5 * field
+    # the overlapped backward holds a second segment of stores, so K = sqrt(nt / 2) = 55
+    assert default_segment(6000, FWI_PSV, 64, g, overlap=True) == 55
+    assert fixed_bytes(6000, FWI_PSV, 64, g, 256, overlap=True) == \
+        (110 * 5 + 2 * 55 * 5 + 2 * 10) * field + 3 * 4 * 64 * 256 * 6000 * 2
+    # no density kernel: a step stores the 3 strain terms only, K = sqrt(5 nt / 3) = 100
+    assert default_segment(6000, FWI_PSV, 64, g, density=False) == 100
+    assert fixed_bytes(6000, FWI_PSV, 64, g, 256, density=False) == \
+        (60 * 5 + 100 * 3 + 2 * 10) * field + 3 * 4 * 64 * 256 * 6000 * 2
     # an explicit segment; the spin state is 6 stress + 2 x 3 velocity/displacement fields,
     # a step stores 6 strain terms and 3 divergences, a batch holds 2 x (6 + 3) + 3 fields
     assert fixed_bytes(100, FWI_SPIN, 2, Grid(8, 8, 1.0, 1.0), 0, segment=10) == \
@@ -149,9 +155,11 @@ def test_max_tail_bytes_is_the_longest_tail_that_fits():
     g = Grid(512, 510, 10.0, 10.0)  # pitch 512
     nt, ns, nrec = 4000, 32, 256
     field = 4 * ns * 512 * 512
-    k = default_segment(nt, FWI_PSV, ns, g)
+    k1 = default_segment(nt, FWI_PSV, ns, g)
+    k2 = default_segment(nt, FWI_PSV, ns, g, overlap=True)
 
     def need(t, segs=1):
+        k = k2 if segs == 2 else k1
         return (math.ceil((nt - t) / k) * 5 + segs * k * 5 + t * 5 + 20) * field + 3 * 4 * ns * nrec * nt * 2
 
     for budget in (30e9, 100e9, 160e9):
