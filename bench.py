@@ -76,7 +76,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
     ap.add_argument("--profile-case", action="store_true",
-                    help="only run a few forward steps (for ncu captures of the step kernel)")
+                    help="only 20 forward steps and one gradient of --nt steps (for ncu captures of the kernels)")
     ap.add_argument("--autotune", action="store_true", help="time every tile variant and report the best")
     ap.add_argument("--overlap", type=int, default=1, choices=[0, 1],
                     help="1: recompute segment s-1 on a second stream while segment s is transposed")
@@ -310,12 +310,22 @@ def main():
     inj = injection_lists(nshots, sid, lambda s: mine[s])
 
     if a.profile_case:
+        # 20 forward steps of the batch, then one exact gradient of nt steps (all of them stored
+        # from the forward sweep): the row-marching step and the transposed step at full size
         b = ShotBatch(m_init, nshots, nt, rid, tile=a.tile)
         d = b.desc(inj=inj, stf=stf)
         b.clear()
         b.run(d, False, 0, min(nt, 20))
+        from seispie_b200.adjoint import ExactAdjoint
+        ea = ExactAdjoint(m_init, nt, sid, lambda s: mine[s], nshots, stf, rid, tail_memory=1e30,
+                          density=bool(a.density))
+        ea.forward()
+        gen = torch.Generator(device=dev).manual_seed(0)
+        g = [torch.randn((nshots, a.nrec, nt), generator=gen, device=dev) if c != 1 else None for c in range(3)]
+        ea.backward(g)
         torch.cuda.synchronize()
-        print(json.dumps({"profile_case": True, "steps": min(nt, 20)}))
+        engine.check_device(None, "profile case")
+        print(json.dumps({"profile_case": True, "forward_steps": min(nt, 20), "gradient_steps": nt}))
         return
 
     # observed data from the checkerboard model (untimed)
