@@ -101,8 +101,8 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
 }
 
 // Untiled bulk copy global -> shared of `bytes` bytes (both addresses 16-byte
-// aligned, bytes a multiple of 16), completion counted on `bar`.  No
-// multicast: the source may be any global memory.
+// aligned, bytes a multiple of 16), completion counted on `bar`; it lands
+// in this CTA's shared memory only, so the source may be any global memory.
 __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
     asm volatile(
         "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
