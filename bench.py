@@ -10,13 +10,18 @@ smoothing sigma 4.  Observed data come from the checkerboard model (computed
 once, untimed).  One step = one gradient of all shots: batched forward with
 checkpoints (row-marching step kernel, no displacement field), misfit and
 trace gradients, exact discrete adjoint (checkpointed recomputation +
-transposed steps with the lambda / mu / rho terms), Gaussian smoothing
+transposed steps with the lambda / mu terms), Gaussian smoothing
 (``--gradient reference``: forward with snapshots and the
 snapshot-correlation adjoint instead).  Cell-updates per step =
 shots * 512 * 512 * 4000 * 2 (forward and adjoint counted separately;
 recomputed forward steps are not counted).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--shard]
+                    [--density 0|1] [--overlap 0|1] [--profile-case]
+
+The gradient is the λ and μ kernels (the reference's gradient is μ); --density 1 adds the ρ
+kernel, whose divergence stores shorten the stored tail.  --overlap 0 runs the backward on one
+stream (recomputation and transposed steps in turn).
 
 On N GPUs (torchrun, one rank per GPU) every rank owns a contiguous block of
 the shots and the ranks sum the FP64 mu kernel and the misfit with one
