@@ -85,6 +85,8 @@ def parse():
     ap.add_argument("--autotune", action="store_true", help="time every tile variant and report the best")
     ap.add_argument("--overlap", type=int, default=1, choices=[0, 1],
                     help="1: recompute segment s-1 on a second stream while segment s is transposed")
+    ap.add_argument("--tail-budget", type=float, default=0.93,
+                    help="fraction of the free HBM the exact gradient's buffers and stored tail may take")
     ap.add_argument("--density", type=int, default=0, choices=[0, 1],
                     help="1: also the density kernel (stores the divergence per step); 0: lambda and mu kernels")
     ap.add_argument("--overlap-ctas", type=int, default=0,
@@ -357,11 +359,11 @@ def main():
         from seispie_b200._lib import FWI_PSV
         from seispie_b200.adjoint import ExactAdjoint, max_tail_bytes
         # per-step stores of the last steps kept from the forward sweep: the longest tail that fits
-        # 90 % of the free HBM with the checkpoints, segment stores, wavefields and traces
+        # --tail-budget of the free HBM with the checkpoints, segment stores, wavefields and traces
         free, _ = torch.cuda.mem_get_info(dev)
         # the mu kernel (the reference's) and the lambda kernel, no density kernel: no divergence stores
-        tail = max_tail_bytes(nt, FWI_PSV, nshots, m_init.grid, 0.9 * free, a.nrec, overlap=bool(a.overlap),
-                              density=bool(a.density))
+        tail = max_tail_bytes(nt, FWI_PSV, nshots, m_init.grid, a.tail_budget * free, a.nrec,
+                              overlap=bool(a.overlap), density=bool(a.density))
         ea = ExactAdjoint(m_init, nt, sid, lambda s: mine[s], nshots, stf, rid, tile=a.tile, tail_memory=tail,
                           overlap=bool(a.overlap), overlap_ctas=a.overlap_ctas, density=bool(a.density))
         checkpointing = {"segment": ea.K, "checkpoints": ea.nseg, "stored_tail_steps": ea.tail,
