@@ -17,11 +17,12 @@ shots * 512 * 512 * 4000 * 2 (forward and adjoint counted separately;
 recomputed forward steps are not counted).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--shard]
-                    [--density 0|1] [--overlap 0|1] [--profile-case]
+                    [--density 0|1] [--overlap 0|1] [--step-overlap 0|1] [--profile-case]
 
 The gradient is the λ and μ kernels (the reference's gradient is μ); --density 1 adds the ρ
 kernel, whose divergence stores shorten the stored tail.  --overlap 0 runs the backward on one
-stream (recomputation and transposed steps in turn).
+stream (recomputation and transposed steps in turn).  --step-overlap 0 launches the steps of the
+forward sweep without programmatic dependent launch.
 
 On N GPUs (torchrun, one rank per GPU) every rank owns a contiguous block of
 the shots and the ranks sum the FP64 mu kernel and the misfit with one
@@ -91,6 +92,9 @@ def parse():
                     help="1: also the density kernel (stores the divergence per step); 0: lambda and mu kernels")
     ap.add_argument("--overlap-ctas", type=int, default=0,
                     help="with --overlap: resident CTAs per SM of the recomputing step (0: all that fit)")
+    ap.add_argument("--step-overlap", type=int, default=1, choices=[0, 1],
+                    help="1: programmatic dependent launch between the steps of a time loop that has the GPU to "
+                         "itself (the forward sweep; the overlapped backward's streams never use it); 0: none")
     ap.add_argument("--shard", action="store_true",
                     help="split the --shots shots over the ranks (strong scaling) instead of --shots per rank")
     ap.add_argument("--gradient", default="exact", choices=["exact", "reference"],
@@ -132,7 +136,8 @@ def config_of(a, w, extra=None, world=1):
          "l2": "inputs larger than L2 (each wavefield field of 32 shots is 32 MiB, the state 5 fields, the "
                "checkpoints and stored steps ~150 GB: far above the 126 MB L2); no flush",
          "parallelism": "shots (contiguous blocks per rank, one FP64 all-reduce per gradient)"
-                        if world > 1 else "shots", "gradient": a.gradient}
+                        if world > 1 else "shots", "gradient": a.gradient,
+         "step_overlap": bool(getattr(a, "step_overlap", 1))}
     if extra:
         c.update(extra)
     return c
@@ -365,7 +370,8 @@ def main():
         tail = max_tail_bytes(nt, FWI_PSV, nshots, m_init.grid, a.tail_budget * free, a.nrec,
                               overlap=bool(a.overlap), density=bool(a.density))
         ea = ExactAdjoint(m_init, nt, sid, lambda s: mine[s], nshots, stf, rid, tile=a.tile, tail_memory=tail,
-                          overlap=bool(a.overlap), overlap_ctas=a.overlap_ctas, density=bool(a.density))
+                          overlap=bool(a.overlap), overlap_ctas=a.overlap_ctas, density=bool(a.density),
+                          step_overlap=bool(a.step_overlap))
         checkpointing = {"segment": ea.K, "checkpoints": ea.nseg, "stored_tail_steps": ea.tail,
                          "overlap": ea.overlap, "overlap_ctas": ea.overlap_ctas}
         kernels = ["lam", "mu"] + (["rho"] if ea.density else [])

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define FWI_ABI_VERSION 6
+#define FWI_ABI_VERSION 7
 
 /* status codes */
 #define FWI_OK 0
@@ -129,6 +129,17 @@ typedef struct fwi_batch {
      * two z columns per thread; 1 = tiles of 32 x 32 cells, one column per
      * thread.  Same adjoint fields bit for bit. */
     int adj_tile;
+    /* 1: programmatic dependent launch between the steps of one fwi_run
+     * (row-marching steps) or fwi_run_transposed (P-SV wide tiles) call --
+     * each step's kernel is scheduled while the previous step is finishing,
+     * hiding launch latency and set-up; every access to the state still
+     * waits for the previous step to complete, so the results are
+     * bit-identical to 0, which serialises the launches.  Worth it for a
+     * time loop that has the GPU to itself; a loop that shares the SMs with
+     * another stream's kernels runs faster with 0 (the early CTAs hold SM
+     * slots while they wait).  No counterpart in the reference (its steps
+     * are separate Numba launches, solver.py:205-234). */
+    int step_overlap;
 } fwi_batch;
 
 /* ABI version of the loaded library (FWI_ABI_VERSION). */

@@ -13,7 +13,7 @@ from . import build as _build
 
 FWI_SH, FWI_PSV, FWI_SPIN = 0, 1, 2
 MODES = {"sh": FWI_SH, "psv": FWI_PSV, "spin": FWI_SPIN}
-ABI_VERSION = 6
+ABI_VERSION = 7
 
 _fp = ctypes.POINTER(ctypes.c_float)
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -36,6 +36,7 @@ class FwiBatch(ctypes.Structure):
         ("seg_e", _vp * 6), ("seg_ds", _vp * 3), ("seg0", ctypes.c_int), ("nseg", ctypes.c_int),
         ("k_nu", _vp), ("k_mnc", _vp), ("k_buoj", _vp), ("rec_order", _vp),
         ("ring", ctypes.c_int), ("ctas_per_sm", ctypes.c_int), ("adj_tile", ctypes.c_int),
+        ("step_overlap", ctypes.c_int),
     ]
 
 

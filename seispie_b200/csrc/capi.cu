@@ -35,8 +35,8 @@ int check_launch(const char *what) {
 int launch_step(const fwi_batch *b, int adjoint, int it, bool snap_u_next, int snap_u_slot, bool snap_v,
                 int snap_v_slot, cudaStream_t st);
 int launch_interaction(const fwi_batch *b, int isae, cudaStream_t st);
-int launch_adjoint_step(const fwi_batch *b, int it, cudaStream_t st);
-int launch_march(const fwi_batch *b, int it, cudaStream_t st);
+int launch_adjoint_step(const fwi_batch *b, int it, bool pdl, cudaStream_t st);
+int launch_march(const fwi_batch *b, int it, bool pdl, cudaStream_t st);
 bool march_supported(const fwi_batch *b);
 int launch_displacement_traces(float *obs, long long ntr, int nt, int it0, int n, double dt, cudaStream_t st);
 int kernel_binary_version(int *v);
@@ -72,6 +72,7 @@ static bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
 static int check_batch(const fwi_batch *b, int adjoint, int it0, int nsteps) {
     REQUIRE(b, "batch is NULL");
     REQUIRE(b->mode == FWI_SH || b->mode == FWI_PSV || b->mode == FWI_SPIN, "mode %d unknown", b->mode);
+    REQUIRE(b->step_overlap == 0 || b->step_overlap == 1, "step_overlap must be 0 or 1 (got %d)", b->step_overlap);
     REQUIRE(b->nx >= 1 && b->nz >= 1, "grid %dx%d is empty", b->nx, b->nz);
     REQUIRE(b->pitch >= b->nz && b->pitch % 4 == 0, "pitch %d must be >= nz (%d) and a multiple of 4", b->pitch,
             b->nz);
@@ -238,8 +239,11 @@ int fwi_run(fwi_batch *b, int adjoint, int it0, int nsteps, void *stream) {
     if (!b->disp[0]) {
         // displacement-free: row-marching steps recording velocity at the
         // receivers, then the traces' running sums over these steps
+        // every launch after the first follows a row-marching step of this loop
+        // directly in the stream, so it may overlap that step's tail
+        const bool pdl = b->step_overlap != 0;
         for (int it = it0; it < it0 + nsteps; it++) {
-            rc = launch_march(b, it, st);
+            rc = launch_march(b, it, pdl && it > it0, st);
             if (rc) return rc;
             b->cur ^= 1;
         }
@@ -315,8 +319,10 @@ int fwi_run_transposed(fwi_batch *b, int it_hi, int nsteps, void *stream) {
         REQUIRE(b->stf[cx] && (b->mode == FWI_SH || b->stf[2]), "fwi_run_transposed: trace gradients (stf) missing");
     }
     cudaStream_t st = (cudaStream_t)stream;
+    // every launch after the first follows a transposed step of this loop directly
+    const bool pdl = b->step_overlap != 0;
     for (int it = it_hi - 1; it >= it_hi - nsteps; it--) {
-        rc = launch_adjoint_step(b, it, st);
+        rc = launch_adjoint_step(b, it, pdl && it < it_hi - 1, st);
         if (rc) return rc;
         b->cur ^= 1;
     }

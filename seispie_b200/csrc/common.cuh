@@ -84,6 +84,26 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
 static inline cudaError_t set_wait_limit_here(int polls) {
     return cudaMemcpyToSymbol(g_wait_polls, &polls, sizeof(int));
 }
+
+// Programmatic dependent launch between consecutive steps of one time loop.
+// A step kernel launched with the ProgrammaticStreamSerialization attribute
+// may be scheduled while the previous step's kernel in the same stream is
+// still running: grid_dep_trigger (at the top of every step kernel) lets the
+// next launch be scheduled once every CTA of this grid has started, and
+// grid_dep_wait blocks the calling thread until the previous grid has
+// completed with all its memory operations visible.  Every access to the
+// wavefields, the stores or the gradient comes after grid_dep_wait; only the
+// barrier set-up and loads of the model (which no step writes) may precede
+// it.  Without the attribute both are no-ops.
+__device__ __forceinline__ void grid_dep_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+
+// Host: the attribute (on for the launches after the first of a time loop
+// whose batch sets fwi_batch.step_overlap).
+inline void set_pdl_attr(cudaLaunchAttribute &at, bool on) {
+    at.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at.val.programmaticStreamSerializationAllowed = on ? 1 : 0;
+}
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int c0, int c1, int c2,
                                             uint64_t *bar) {
     asm volatile(

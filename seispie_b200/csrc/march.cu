@@ -172,11 +172,15 @@ __global__ void __launch_bounds__(kMaxPitch / 4, 2) march_kernel(const __grid_co
     auto ring_row = [&](int slot, int f) -> float * { return smem + (slot * NF + f) * RL + 4; };
 
 
+    grid_dep_trigger();
     if (tid == 0) {
         for (int i = 0; i < N; i++) mbar_init(&full[i], 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     __syncthreads();
+    // the previous step (state rows, and the stress / velocity buffers this
+    // step overwrites) is complete from here on
+    grid_dep_wait();
 
     // thread 0: stream row q of the shot at soff into the slot of sequence number sn
     auto issue = [&](long long soff, int q, int sn) {
@@ -703,7 +707,7 @@ static int march_choose(int nthr, int rl, int want, int *n_out, size_t *bytes_ou
 }
 
 template <int MODE, int N>
-static int launch_march_mode(const MarchArgs &a, int nthr, size_t bytes, int occ, cudaStream_t st) {
+static int launch_march_mode(const MarchArgs &a, int nthr, size_t bytes, int occ, bool pdl, cudaStream_t st) {
     static int sms = 0;
     if (!sms) {
         int dev = 0;
@@ -712,11 +716,21 @@ static int launch_march_mode(const MarchArgs &a, int nthr, size_t bytes, int occ
             sms = 148;
     }
     const long long grid = a.rows_total < (long long)sms * occ ? a.rows_total : (long long)sms * occ;
-    march_kernel<MODE, N><<<(unsigned)grid, nthr, bytes, st>>>(a);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid, 1, 1);
+    cfg.blockDim = dim3(nthr, 1, 1);
+    cfg.dynamicSmemBytes = bytes;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    set_pdl_attr(attr[0], true);
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, march_kernel<MODE, N>, a);
+    if (e != cudaSuccess) return set_error(FWI_ECUDA, "march_kernel launch: %s", cudaGetErrorString(e));
     return check_launch("march_kernel");
 }
 
-int launch_march(const fwi_batch *b, int it, cudaStream_t st) {
+int launch_march(const fwi_batch *b, int it, bool pdl, cudaStream_t st) {
     MarchArgs a;
     const int mode = b->mode;
     a.nx = b->nx;
@@ -773,17 +787,17 @@ int launch_march(const fwi_batch *b, int it, cudaStream_t st) {
     if (b->ctas_per_sm > 0 && b->ctas_per_sm < occ) occ = b->ctas_per_sm;
     if (mode == FWI_SH) {
         switch (n) {
-            case 3: return launch_march_mode<FWI_SH, 3>(a, nthr, bytes, occ, st);
-            case 4: return launch_march_mode<FWI_SH, 4>(a, nthr, bytes, occ, st);
-            case 6: return launch_march_mode<FWI_SH, 6>(a, nthr, bytes, occ, st);
-            default: return launch_march_mode<FWI_SH, 8>(a, nthr, bytes, occ, st);
+            case 3: return launch_march_mode<FWI_SH, 3>(a, nthr, bytes, occ, pdl, st);
+            case 4: return launch_march_mode<FWI_SH, 4>(a, nthr, bytes, occ, pdl, st);
+            case 6: return launch_march_mode<FWI_SH, 6>(a, nthr, bytes, occ, pdl, st);
+            default: return launch_march_mode<FWI_SH, 8>(a, nthr, bytes, occ, pdl, st);
         }
     }
     switch (n) {
-        case 3: return launch_march_mode<FWI_PSV, 3>(a, nthr, bytes, occ, st);
-        case 4: return launch_march_mode<FWI_PSV, 4>(a, nthr, bytes, occ, st);
-        case 6: return launch_march_mode<FWI_PSV, 6>(a, nthr, bytes, occ, st);
-        default: return launch_march_mode<FWI_PSV, 8>(a, nthr, bytes, occ, st);
+        case 3: return launch_march_mode<FWI_PSV, 3>(a, nthr, bytes, occ, pdl, st);
+        case 4: return launch_march_mode<FWI_PSV, 4>(a, nthr, bytes, occ, pdl, st);
+        case 6: return launch_march_mode<FWI_PSV, 6>(a, nthr, bytes, occ, pdl, st);
+        default: return launch_march_mode<FWI_PSV, 8>(a, nthr, bytes, occ, pdl, st);
     }
 }
 

@@ -1677,6 +1677,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 #pragma unroll
         for (int q = 0; q < T::NV; q++) tma_load_3d(sV + q * FV, &m.vel[q], z0 - 4, x0 - 1, shot, &bar[2]);
     };
+    grid_dep_trigger();
     if (tid == 0) {
 #pragma unroll
         for (int b = 0; b < 3; b++) mbar_init(&bar[b], 1);
@@ -1684,15 +1685,19 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
     __syncthreads();
     if (tid == 0) {
+        // the model tile (no step writes it) streams in while the previous
+        // step may still be running
         mbar_expect_tx(&bar[0], T::model_bytes);
 #pragma unroll
         for (int f = 0; f < 2; f++) tma_load_2d(sL + f * FS, &m.lm[f], z0 - 4, x0 - 3, &bar[0]);
 #pragma unroll
         for (int p = 0; p < 2; p++) tma_load_2d(sP + p * FV, &m.vp[p], z0 - 4, x0 - 1, &bar[0]);
-        if (crank < nshots) {
-            issue_sig(crank);
-            issue_vel(crank);
-        }
+    }
+    // the previous step (adjoint state, gradient sums) is complete from here on
+    grid_dep_wait();
+    if (tid == 0 && crank < nshots) {
+        issue_sig(crank);
+        issue_vel(crank);
     }
 
     float2 gk[T::NK][RPW];
@@ -2082,7 +2087,7 @@ static int launch_adjoint(const fwi_batch *b, const AdjArgs &a, cudaStream_t st)
     return check_launch("adjoint_kernel");
 }
 
-static int launch_adjoint_wide(const fwi_batch *b, const AdjArgs &a, cudaStream_t st) {
+static int launch_adjoint_wide(const fwi_batch *b, const AdjArgs &a, bool pdl, cudaStream_t st) {
     using T = WideTile;
     static bool set = false;
     if (!set) {
@@ -2101,13 +2106,14 @@ static int launch_adjoint_wide(const fwi_batch *b, const AdjArgs &a, cudaStream_
     cfg.blockDim = dim3(kThreads, 1, 1);
     cfg.dynamicSmemBytes = T::bytes;
     cfg.stream = st;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = 1;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = C;
+    set_pdl_attr(attr[1], true);
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = pdl ? 2 : 1;
     cudaError_t e = cudaLaunchKernelEx(&cfg, adjoint_wide_kernel, a, m);
     if (e != cudaSuccess) return set_error(FWI_ECUDA, "adjoint_wide_kernel launch: %s", cudaGetErrorString(e));
     return check_launch("adjoint_wide_kernel");
@@ -2115,7 +2121,7 @@ static int launch_adjoint_wide(const fwi_batch *b, const AdjArgs &a, cudaStream_
 
 // One transposed step (forward step `it`, adjoint state it+1 -> it) with
 // its gradient terms.
-int launch_adjoint_step(const fwi_batch *b, int it, cudaStream_t st) {
+int launch_adjoint_step(const fwi_batch *b, int it, bool pdl, cudaStream_t st) {
     AdjArgs a;
     a.nx = b->nx;
     a.nz = b->nz;
@@ -2165,7 +2171,7 @@ int launch_adjoint_step(const fwi_batch *b, int it, cudaStream_t st) {
     a.g[1] = mode == FWI_SH ? nullptr : b->stf[2];
     switch (mode) {
         case FWI_SH: return launch_adjoint<FWI_SH>(b, a, st);
-        case FWI_PSV: return b->adj_tile == 1 ? launch_adjoint<FWI_PSV>(b, a, st) : launch_adjoint_wide(b, a, st);
+        case FWI_PSV: return b->adj_tile == 1 ? launch_adjoint<FWI_PSV>(b, a, st) : launch_adjoint_wide(b, a, pdl, st);
         default: return launch_adjoint<FWI_SPIN>(b, a, st);
     }
 }

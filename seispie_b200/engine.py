@@ -207,6 +207,8 @@ class ShotBatch:
         self.ring = 0  # staging-ring depth of the row-marching kernel (0 = automatic)
         self.ctas_per_sm = 0  # row-marching grid: resident CTAs per SM (0 = all that fit)
         self.adj_tile = 0  # P-SV transposed step: 0 = 32 x 64 tiles, 1 = 32 x 32 tiles
+        # programmatic dependent launch between the steps of one call (fwi_batch.step_overlap)
+        self.step_overlap = 1
 
     # ------------------------------------------------------------ descriptors
     def desc(self, inj=None, stf=(None, None, None), record=True, kernels=(None, None, None)) -> FwiBatch:
@@ -217,6 +219,7 @@ class ShotBatch:
         b.nshots, b.nt, b.dx, b.dz, b.dt = self.nshots, self.nt, float(g.dx), float(g.dz), float(m.dt)
         b.cur, b.tile, b.ring, b.ctas_per_sm = self.cur, self.tile, self.ring, self.ctas_per_sm
         b.adj_tile = self.adj_tile
+        b.step_overlap = self.step_overlap
         for h in range(2):
             for f, t in enumerate(self.sig[h]):
                 b.sig[h][f] = ptr(t)

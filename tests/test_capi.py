@@ -64,6 +64,7 @@ def _batch(**kw):
 
 @pytest.mark.parametrize("kw,msg", [
     (dict(mode=7), "mode"),
+    (dict(step_overlap=2), "step_overlap"),
     (dict(pitch=18), "pitch"),
     (dict(pitch=12), "pitch"),
     (dict(nshots=0), "nshots"),
@@ -110,3 +111,4 @@ def test_wait_limit_rejects_negative_before_any_cuda_call():
     assert lib.fwi_set_wait_limit(-5) == -1
     code, msg = _err()
     assert code == -1 and "polls" in msg
+
