@@ -31,11 +31,16 @@ all-reduce before the smoothing, as the reference sums before it smooths
 with N: weak scaling); ``--shard`` splits the 32 shots over the ranks
 (strong scaling).
 
-Prints one JSON line (rank 0).  ``value`` is measured with every input in HBM;
+Prints one JSON line (rank 0).  ``value`` is measured with every input in HBM,
+on the exact gradient captured once in a CUDA graph and replayed per step
+(seispie_b200.adjoint.GradientGraph: one host launch per gradient; the
+all-reduce and the smoothing run eagerly); ``eager`` holds the same gradient
+launched step by step, whose CUDA events time the roofline's kernel
+(``--graph 0`` makes the step-by-step gradient the value);
 ``e2e`` through the plugin API (seispie_b200.solver.b200.compute_gradient)
 with the observed traces in host memory, their upload and the gradient's
 download inside the timed region.  ``roofline`` is the row-marching step
-kernel's (CUDA events around its launches inside the timed region);
+kernel's (CUDA events around its launches inside the eager timed region);
 ``gradient_roofline`` the whole gradient's useful cell-update rate in the
 same bytes.  ``--impl reference`` times the CPU restatement of the
 reference's arithmetic (oracle/, float32, all host threads) on a bounded
@@ -95,6 +100,10 @@ def parse():
     ap.add_argument("--step-overlap", type=int, default=1, choices=[0, 1],
                     help="1: programmatic dependent launch between the steps of a time loop that has the GPU to "
                          "itself (the forward sweep; the overlapped backward's streams never use it); 0: none")
+    ap.add_argument("--graph", type=int, default=1, choices=[0, 1],
+                    help="1: value is the exact gradient captured in one CUDA graph (forward sweep, misfit and "
+                         "backward replayed as one launch per gradient; the step-by-step gradients that carry the "
+                         "roofline's events are reported under 'eager'); 0: value is the step-by-step gradient")
     ap.add_argument("--shard", action="store_true",
                     help="split the --shots shots over the ranks (strong scaling) instead of --shots per rank")
     ap.add_argument("--gradient", default="exact", choices=["exact", "reference"],
@@ -137,7 +146,8 @@ def config_of(a, w, extra=None, world=1):
                "checkpoints and stored steps ~150 GB: far above the 126 MB L2); no flush",
          "parallelism": "shots (contiguous blocks per rank, one FP64 all-reduce per gradient)"
                         if world > 1 else "shots", "gradient": a.gradient,
-         "step_overlap": bool(getattr(a, "step_overlap", 1))}
+         "step_overlap": bool(getattr(a, "step_overlap", 1)),
+         "cuda_graph": bool(getattr(a, "graph", 0)) and a.gradient == "exact"}
     if extra:
         c.update(extra)
     return c
@@ -461,6 +471,52 @@ def main():
         dist.barrier()
     cells = 2 * ntot * nx * nz * nt  # useful cell-updates of the whole job per step
     value = cells / (ms * 1e-3) / 1e9
+    misfit_total = float(mis.item())
+
+    # The headline: the same gradient captured in one CUDA graph (forward sweep, misfit, backward) and
+    # replayed, one launch per gradient from the host; the eager gradients above, launched step by step,
+    # carry the per-launch CUDA events of the roofline.
+    eager = None
+    if a.gradient == "exact" and a.graph:
+        from seispie_b200.adjoint import GradientGraph
+
+        def between(tr):
+            return grads, [engine.misfit_tracegrad(data[c], tr[c].reshape(-1), grads[c], nshots, a.nrec, nt, dt)
+                           for c in (0, 2)]
+
+        ea.step_events = None  # no per-segment events inside the graph
+        gg = GradientGraph(ea, between)
+        for _ in range(a.warmup):
+            _, gm, gk = gg.replay()
+            reduce_and_smooth(gm, gk[1])
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        eager = {"value": value, "ms_per_step": ms, "gpu_launches": launches, "clocks": clk.summary(),
+                 "note": "the same gradients launched step by step from the host (the roofline's CUDA events)"}
+        launches0 = lib.fwi_launch_count()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            torch.cuda.synchronize()
+            g0.record(stream)
+            for _ in range(a.steps):
+                _, gm, gk = gg.replay()
+                gmis, _ = reduce_and_smooth(gm, gk[1])
+            g1.record(stream)
+            torch.cuda.synchronize()
+        # library kernels of the replays (counted once, at capture) plus the smoothing launched eagerly
+        launches = gg.launches * a.steps + lib.fwi_launch_count() - launches0
+        ms = g0.elapsed_time(g1) / a.steps
+        engine.check_device(stream, "bench (graph)")
+        eager["graph_misfit_equal"] = float(gmis.item()) == misfit_total  # bit for bit
+        if world > 1:
+            tt = torch.tensor([ms], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms = float(tt.item())
+            dist.barrier()
+        value = cells / (ms * 1e-3) / 1e9
+        eager["graph_nodes_library_kernels"] = gg.launches
+        del gg
 
     peak, peak_src = 6650.0, "fallback"
     try:
@@ -505,7 +561,7 @@ def main():
     grad_roof = {"bytes_per_cell_update": 72, "achieved": value / world * 72, "peak": peak, "unit": "GB/s",
                  "frac": value / world * 72 / peak,
                  "basis": "useful forward+adjoint cell-updates (recomputed steps not counted) x 72 B"}
-    misfit_total = float(mis.item())
+
     del b, fwd, adj
     ea = grads = None  # noqa: F841  (release the checkpoint buffers before the e2e run)
     torch.cuda.empty_cache()
@@ -532,7 +588,7 @@ def main():
                 "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
                 "scaling": "strong" if a.shard else "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic", "config": config_of(a, w, extra, world), "clocks": clk.summary(),
-                "gpu_launches": launches, "roofline": roof, "gradient_roofline": grad_roof, "e2e": e2e,
+                "gpu_launches": launches, "roofline": roof, "gradient_roofline": grad_roof, "eager": eager, "e2e": e2e,
                 "cpu_baseline": cpu, "reference_cudasim": reference_cudasim() if cpu else None, "impl": "b200"}
         print(json.dumps(line), flush=True)
     if world > 1:

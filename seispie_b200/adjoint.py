@@ -212,6 +212,8 @@ class ExactAdjoint:
         if self.overlap:
             self.seg_e2 = [None if t is None else torch.empty_like(t) for t in self.seg_e]
             self.seg_ds2 = [None if t is None else torch.empty_like(t) for t in self.seg_ds]
+        self._adj = None  # adjoint batch and its injection lists (made by the first backward)
+        self._side = None  # the overlapped backward's recomputing stream
         self.tail_e, self.tail_ds = [None] * 6, [None, None, None]
         if self.tail:
             for k in range(strain_fields(self.mode)):
@@ -279,12 +281,11 @@ class ExactAdjoint:
                 # u~ at the receivers: suffix sums of dL/d(trace) over time
                 g = g_traces[c].to(torch.float32).contiguous()
                 stf[c] = engine.trace_suffix_sum(g, torch.empty_like(g)).reshape(-1)
-        adj = ShotBatch(self.model, self.nshots, self.nt, self.rec_id)
+        adj, inj = self._adjoint_batch()
         adj.adj_tile = self.adj_tile
         # the overlapped backward's streams share the SMs: no early launches there
         adj.step_overlap = 0 if self.overlap else self.step_overlap
         adj.clear()
-        inj = adjoint_injection_lists(self.nshots, self.rec_id) if len(self.rec_id) else None
         adesc = adj.desc(inj=inj, stf=stf, record=False, kernels=k)
         fwd = self.fwd
 
@@ -323,6 +324,18 @@ class ExactAdjoint:
         fwd.set_segment(self.rdesc, [None] * 6, [None] * 3, 0, 0)
         return tuple(k)
 
+    def _adjoint_batch(self):
+        """The adjoint batch and its receiver injection lists (on the
+        device), made by the first backward and kept, so that later
+        backwards make no host-to-device copy (and can be captured in a
+        CUDA graph)."""
+        if self._adj is None:
+            adj = ShotBatch(self.model, self.nshots, self.nt, self.rec_id)
+            inj = (engine.upload_lists(adjoint_injection_lists(self.nshots, self.rec_id), self.model.device)
+                   if len(self.rec_id) else None)
+            self._adj = (adj, inj)
+        return self._adj
+
     def _backward_overlapped(self, adj: ShotBatch, adesc) -> None:
         """The levels = 1 backward with the recomputation one segment ahead
         on a second stream: segment s-1 is recomputed into one store buffer
@@ -334,7 +347,9 @@ class ExactAdjoint:
         priorities and 54.5 the other way round)."""
         fwd = self.fwd
         main = torch.cuda.current_stream() if adj.stream is None else adj.stream
-        side = torch.cuda.Stream(device=self.model.device, priority=torch.cuda.Stream.priority_range()[1])
+        if self._side is None:
+            self._side = torch.cuda.Stream(device=self.model.device, priority=torch.cuda.Stream.priority_range()[1])
+        side = self._side
         side.wait_stream(main)  # the forward sweep and the trace sums
         bufs = ((self.seg_e, self.seg_ds), (self.seg_e2, self.seg_ds2))
         freed = [None, None]  # per buffer: event after the last transposes that read it
@@ -383,6 +398,74 @@ def _pad(t: torch.Tensor, grid: Grid) -> torch.Tensor:
     out = torch.zeros((grid.nx, grid.pitch), dtype=torch.float32, device=t.device)
     out[:, : grid.nz] = t.reshape(grid.nx, grid.nz)
     return out
+
+
+class GradientGraph:
+    """One exact gradient -- the checkpointed forward sweep, the caller's
+    misfit step and the backward -- captured in two CUDA graphs that share
+    one memory pool, so that a gradient of all shots of the batch is two
+    launches from the host (its thousands of step kernels, copies and the
+    overlapped backward's two streams become graph nodes; the
+    programmatic-dependent-launch edges of the forward sweep are kept).
+    The split lets a caller upload the observed traces that the misfit step
+    reads while the forward sweep runs.
+
+    ``between(traces)`` enqueues the misfit work on the current stream and
+    returns (trace gradients per component slot, extra outputs); it must
+    neither synchronise nor copy from host memory.  Construction runs one
+    eager gradient first (it makes the adjoint batch and fills the
+    library's launch caches; ``warm_up=False`` skips it when ``ea`` has
+    just computed one) and then captures one, on the model's stream when it
+    has one.  ``replay()`` (or ``replay_forward()`` then
+    ``replay_backward()``) computes the gradient for the model's current
+    values (update the model tensors in place between replays) on the
+    current stream and returns (traces, extra, kernels): tensors owned by
+    the graphs that the next replay overwrites.  The values are those of
+    the eager ExactAdjoint.forward / backward, bit for bit.  ``launches`` is
+    the number of library kernels one gradient runs."""
+
+    def __init__(self, ea: ExactAdjoint, between, warm_up: bool = True):
+        self.ea = ea
+        if ea.step_events is not None:
+            raise ValueError("GradientGraph: step events cannot be recorded inside a graph")
+        dev = ea.model.device
+        stream = ea.model.stream  # the batches' stream (None: the current one)
+        if warm_up:
+            main = torch.cuda.current_stream(dev)
+            warm = stream if stream is not None else torch.cuda.Stream(device=dev)
+            warm.wait_stream(main)
+            with torch.cuda.stream(warm):
+                g, _ = between(ea.forward())
+                ea.backward(g)
+            main.wait_stream(warm)
+        lib = engine._lib.load()
+        n0 = lib.fwi_launch_count()
+        self.forward_graph, self.backward_graph = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+        # thread_local: host threads that stage data meanwhile do not void the capture
+        with torch.cuda.graph(self.forward_graph, stream=stream, capture_error_mode="thread_local"):
+            self.traces = ea.forward()
+        with torch.cuda.graph(self.backward_graph, pool=self.forward_graph.pool(), stream=stream,
+                              capture_error_mode="thread_local"):
+            g, self.extra = between(self.traces)
+            self.kernels = ea.backward(g)
+        self.launches = lib.fwi_launch_count() - n0
+        self.illum = ea.illum
+
+    def replay_forward(self):
+        """The forward sweep; returns the traces."""
+        self.forward_graph.replay()
+        return self.traces
+
+    def replay_backward(self):
+        """The misfit step and the backward of the last forward sweep;
+        returns (extra, kernels)."""
+        self.backward_graph.replay()
+        return self.extra, self.kernels
+
+    def replay(self):
+        self.replay_forward()
+        self.replay_backward()
+        return self.traces, self.extra, self.kernels
 
 
 class Seismograms(torch.autograd.Function):

@@ -232,7 +232,7 @@ class ShotBatch:
         if self.mode == FWI_SPIN:
             b.buo_j, b.nu, b.mnc = ptr(m.buo_j), ptr(m.nu), ptr(m.mnc)
         if inj is not None:
-            ip, ic, ir = (torch.as_tensor(np.asarray(a, dtype=np.int32)).to(self.device) for a in inj)
+            ip, ic, ir = upload_lists(inj, self.device)
             b._keep = [ip, ic, ir]
             b.inj_ptr, b.inj_cell, b.inj_row = ptr(ip), ptr(ic), ptr(ir)
             for c in range(3):
@@ -334,6 +334,14 @@ def injection_lists(nshots: int, src_id: np.ndarray, isrc_of_shot) -> tuple:
             row.append(int(i))
         ptr_.append(len(cell))
     return _sort_by_cell(np.asarray(ptr_, np.int32), np.asarray(cell, np.int32), np.asarray(row, np.int32))
+
+
+def upload_lists(inj, device) -> tuple:
+    """Injection lists (ptr, cell, row) as int32 device tensors; lists that
+    are device tensors already are passed through (no host copy, so a
+    descriptor built from them can be made during CUDA-graph capture)."""
+    return tuple(a if isinstance(a, torch.Tensor) and a.is_cuda else
+                 torch.as_tensor(np.asarray(a, dtype=np.int32)).to(device) for a in inj)
 
 
 def adjoint_injection_lists(nshots: int, rec_id: np.ndarray) -> tuple:

@@ -137,6 +137,7 @@ class b200:
     def import_sources(self):
         """fd2d.py:122-146: src_id by round-half-even of x/dx and z/dz; the
         Ricker time functions are evaluated on the device (fwi_ricker)."""
+        self._drop_graphs()
         src = np.loadtxt(self.path["sources"], ndmin=2)
         self.nsrc = src.shape[0]
         self.src = src
@@ -147,6 +148,7 @@ class b200:
 
     def import_stations(self):
         """fd2d.py:148-165."""
+        self._drop_graphs()
         rec = np.loadtxt(self.path["stations"], ndmin=2)
         self.nrec = rec.shape[0]
         self.rec = rec
@@ -162,6 +164,7 @@ class b200:
     def import_model(self, model_true):
         """fd2d.py:167-252: read proc000000_<name>.bin, infer the grid, set
         lambda/mu (vps2lm) and the sponge (set_bound) on the device."""
+        self._drop_graphs()
         model = dict()
         model_dir = self.path["model_true"] if model_true else self.path["model_init"]
         names = (["x", "z", "lambda", "mu", "nu", "j", "lambda_c", "mu_c", "nu_c", "rho"] if self.spin
@@ -264,11 +267,47 @@ class b200:
             return g == "exact"
         return mode == FWI_PSV
 
+    def _graph_key(self, mode, shots):
+        """What a captured gradient depends on besides the values of the
+        model, the observed traces and the time functions: the batch, the
+        device buffers the graph reads and the settings of the step loops.
+        None when no graph is kept (cuda_graph = no, or batch_memory_gb caps
+        the memory of a batch)."""
+        if self.config.get("cuda_graph", "yes") != "yes" or self.batch_memory > 0:
+            return None
+        m = self.model
+        names = ("rho", "lam", "mu", "bound", "buo", "nu", "j", "mu_c", "nu_c", "buo_j", "mnc")
+        bufs = tuple(getattr(m, n).data_ptr() for n in names if getattr(m, n, None) is not None) + \
+            tuple(t.data_ptr() for t in (self.stf_x, self.stf_y, self.stf_z))
+        return (mode, tuple(shots), self.config["combine_sources"], self.nt, self.dt, self.tile,
+                self._density(mode), tuple(np.asarray(self.src_id).tolist()),
+                tuple(np.asarray(self.rec_id).tolist()), bufs)
+
+    def _drop_graphs(self):
+        """Release a kept gradient graph and the batch it holds (a new
+        model, sources or stations make it stale)."""
+        if getattr(self, "_graphs", None):
+            self._graphs.clear()
+            torch.cuda.empty_cache()
+
     def _exact_gradient(self, mode, shots, data_of) -> float:
         """Misfit and exact gradient of this process's shots, accumulated in
         the reference's units (dt * dchi/dparam) into k_lam_f64 / k_mu_f64 /
-        k_rho_f64; returns the misfit (sum of per-shot, per-component norms)."""
-        from ..adjoint import ExactAdjoint, max_tail_bytes
+        k_rho_f64; returns the misfit (sum of per-shot, per-component norms).
+
+        With all shots in one batch (the default when they fit), the first
+        call computes the gradient eagerly and then captures it in a CUDA
+        graph (seispie_b200.adjoint.GradientGraph) that it keeps with the
+        batch's buffers; later calls with the same shots, model buffers and
+        settings upload the observed traces into the graph's input buffers
+        and replay it: one launch per gradient, the same values bit for bit.
+        Any other call drops the kept graph first."""
+        from ..adjoint import ExactAdjoint, GradientGraph, max_tail_bytes
+        key = self._graph_key(mode, shots)
+        kept = self.__dict__.setdefault("_graphs", {})
+        if key is not None and key in kept:
+            return self._replay_gradient(mode, shots, data_of, kept[key])
+        self._drop_graphs()  # release a kept batch before this one is sized
         combine = self.config["combine_sources"] == "yes"
         misfit = 0.0
         nrec, nt = self.nrec, self.nt
@@ -303,7 +342,53 @@ class b200:
                     misfit += float(engine.misfit_tracegrad(data, syn, grads[c], n, nrec, nt, self.dt).sum().item())
                     grads[c] = grads[c].view(n, nrec, nt)
                 self._accumulate_exact(mode, ea.backward(grads))
+                if key is not None and list(chunk) == list(shots):
+                    # keep the batch and capture its gradient for the next calls; the uploaded
+                    # traces become the graph's input buffers
+                    kept[key] = (GradientGraph(ea, self._misfit_step(data_of, uploads, n), warm_up=False), uploads)
                 del ea
+        return misfit
+
+    def _misfit_step(self, data_of, inputs, n):
+        """The misfit step of a captured gradient: trace gradients and
+        per-shot misfits of every component slot against the observed
+        traces in the device buffers `inputs`."""
+        nrec, nt = self.nrec, self.nt
+
+        def between(tr):
+            grads, mis = [None, None, None], []
+            for slot, (c, lst) in enumerate(data_of):
+                g = torch.empty(n * nrec * nt, dtype=torch.float32, device=self.device)
+                mis.append(engine.misfit_tracegrad(inputs[slot], tr[c].reshape(-1).contiguous(), g, n, nrec, nt,
+                                                   self.dt))
+                grads[c] = g.view(n, nrec, nt)
+            return grads, mis
+        return between
+
+    def _replay_gradient(self, mode, shots, data_of, entry) -> float:
+        """A kept gradient graph: the forward sweep replays while the
+        observed traces of this call are stacked into pinned memory (worker
+        threads) and uploaded into the graph's input buffers (copy stream);
+        then the misfit and backward replay and the kernels accumulate as on
+        the eager path."""
+        gg, inputs = entry
+        staged = self._stage(data_of, shots, shots)
+        with self._ctx():
+            gg.replay_forward()
+        copy = self._copy_stream()
+        # the previous call's misfit step has read the inputs: that call ended with a host read
+        # of its misfit, which followed it on the device
+        with torch.cuda.stream(copy):
+            for buf, f in zip(inputs, staged):
+                buf.copy_(f.result().reshape(buf.shape), non_blocking=True)
+        self.stream.wait_stream(copy)
+        with self._ctx():
+            mis, ks = gg.replay_backward()
+            self.illum_f64 += gg.illum
+            misfit = 0.0
+            for m in mis:
+                misfit += float(m.sum().item())
+            self._accumulate_exact(mode, ks)
         return misfit
 
     def _accumulate_exact(self, mode, ks):

@@ -499,3 +499,133 @@ def test_step_overlap_is_bit_identical(mode):
             assert (a is None and b is None) or torch.equal(a, b)
         assert torch.equal(il1, il2)
 
+
+@pytest.mark.parametrize("overlap", [False, True])
+def test_gradient_graph_is_bit_identical(overlap):
+    """One exact gradient (forward sweep, misfit and trace gradients,
+    backward) captured in one CUDA graph and replayed: traces, misfit,
+    every gradient term and the illumination equal the eager run's bit for
+    bit, on two replays in a row and again after the model tensors have been
+    changed in place (the graph reads the model's current values)."""
+    from seispie_b200 import engine
+    from seispie_b200.adjoint import AcquisitionSetup, ExactAdjoint, GradientGraph
+    from seispie_b200.engine import Grid, build_model
+    nx, nz, nt, h, dt = 96, 130, 240, 10.0, 1e-3
+    rng = np.random.default_rng(12)
+    src = np.array([[120.0 + 150 * s, 150.0 + 70 * (s % 3), 0, 14.0, 0.07, 25.0, 1e10] for s in range(4)])
+    rec = np.array([[50.0 + 37 * r, 30.0 + 40 * (r % 3)] for r in range(23)])
+    absorb = (8, 0.05, 1, 1, 1, 0)
+    grid = Grid(nx, nz, h, h)
+    setup = AcquisitionSetup("psv", grid, dt, nt, src, rec, absorb)
+    npt = nx * nz
+    prm = dict(rho=np.full(npt, 2700.0) * (1 + 0.05 * rng.random(npt)),
+               lam=np.full(npt, 8.1e9) * (1 + 0.05 * rng.random(npt)),
+               mu=np.full(npt, 8.1e9) * (1 + 0.05 * rng.random(npt)))
+    m = build_model("psv", grid, dt, prm, absorb, "cuda")
+    nrec, ns = len(setup.rec_id), setup.nshots
+    data = [torch.randn(ns * nrec * nt, device="cuda") * 1e-9 if c != 1 else None for c in range(3)]
+    grads = [torch.empty((ns, nrec, nt), device="cuda") if c != 1 else None for c in range(3)]
+    per_step = 3 * 4 * ns * nx * grid.pitch
+
+    def make():
+        return ExactAdjoint(m, nt, setup.src_id, setup.isrc_of_shot, ns, setup.stf, setup.rec_id, segment=23,
+                            tail_memory=41.5 * per_step, overlap=overlap, density=False)
+
+    def between(tr):
+        mis = [engine.misfit_tracegrad(data[c], tr[c].reshape(-1), grads[c], ns, nrec, nt, dt) for c in (0, 2)]
+        return grads, torch.stack(mis)
+
+    def eager():
+        ea = make()
+        tr = ea.forward()
+        g, mis = between(tr)
+        k = ea.backward(g)
+        torch.cuda.synchronize()
+        return [t.clone() if t is not None else None for t in tr], mis.clone(), k, ea.illum.clone()
+
+    def same(x, y):
+        (tr1, m1, k1, i1), (tr2, m2, k2, i2) = x, y
+        for a, b in zip(tr1, tr2):
+            assert (a is None and b is None) or torch.equal(a, b)
+        assert torch.equal(m1, m2)
+        for a, b in zip(k1, k2):
+            assert (a is None and b is None) or torch.equal(a, b)
+        assert torch.equal(i1, i2)
+
+    ref = eager()
+    assert float(ref[2][1].abs().max()) > 0 and float(ref[1].sum()) > 0
+    gg = GradientGraph(make(), between)
+    assert gg.launches > 2 * nt  # every forward, recomputed and transposed step is a node
+    for _ in range(2):
+        tr, mis, k = gg.replay()
+        torch.cuda.synchronize()
+        same(ref, ([t.clone() if t is not None else None for t in tr], mis.clone(), k, gg.illum.clone()))
+    m.mu.mul_(1.02)
+    m.lam.mul_(0.99)
+    ref2 = eager()
+    assert not torch.equal(ref2[2][1], ref[2][1])
+    tr, mis, k = gg.replay()
+    torch.cuda.synchronize()
+    same(ref2, ([t.clone() if t is not None else None for t in tr], mis.clone(), k, gg.illum.clone()))
+
+
+def _psv_plugin(root, **over):
+    """A b200 plugin on a small P-SV checkerboard case (observed traces
+    imported from the true model, the initial model loaded)."""
+    import os
+    from seispie_b200.io import write_model
+    from seispie_b200.solver import b200
+    nx, nz, h, nt = 44, 38, 10.0, 240
+    i, j = np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij")
+    vs_true = 1732 * (1 + 0.05 * np.sign(np.sin(i / 5.0) * np.sin(j / 5.0) + 1e-9))
+    for d, vs in (("true", vs_true.ravel()), ("init", np.full(nx * nz, 1732.0))):
+        if not os.path.isdir(os.path.join(root, d)):
+            write_model(os.path.join(root, d), nx, nz, h, h, dict(vp=np.full(nx * nz, 3000.0), vs=vs,
+                                                                  rho=np.full(nx * nz, 2600.0)))
+    src = np.array([[100.0, 60.0, 0, 14.0, 0.07, 20.0, 1e10], [300.0, 60.0, 0, 14.0, 0.07, -30.0, 1e10],
+                    [200.0, 90.0, 0, 14.0, 0.07, 10.0, 1e10]])
+    rec = np.array([[30.0 + 30 * r, 80.0] for r in range(12)])
+    np.savetxt(os.path.join(root, "src.dat"), src)
+    np.savetxt(os.path.join(root, "rec.dat"), rec)
+    os.makedirs(os.path.join(root, "out"), exist_ok=True)
+    s = b200()
+    s.config = dict(nt=str(nt), dt="1e-3", sh="no", psv="yes", abs_left="yes", abs_right="yes", abs_top="no",
+                    abs_bottom="yes", abs_width="8", abs_alpha="0.05", save_coordinates="", combine_sources="no",
+                    save_snapshot="0", adjoint_interval="4", smooth="2")
+    s.config.update(over)
+    s.path = dict(model_true=os.path.join(root, "true"), model_init=os.path.join(root, "init"),
+                  sources=os.path.join(root, "src.dat"), stations=os.path.join(root, "rec.dat"),
+                  output=os.path.join(root, "out"))
+    s.mpi = None
+    s.setup(None)
+    s.import_model(1)
+    s.import_sources()
+    s.import_stations()
+    s.import_traces()
+    s.import_model(0)
+    return s
+
+
+def test_plugin_gradient_graph_replays_bit_identical(tmp_path):
+    """compute_gradient of the plugin keeps the exact gradient of its shots
+    in a CUDA graph after the first call and replays it on the next ones:
+    misfits and the FP64 lambda / mu kernels equal those of a plugin that
+    never captures (cuda_graph = no) bit for bit, over three gradients with
+    the model changed in place between them; a new model drops the graph."""
+    a = _psv_plugin(str(tmp_path))
+    b = _psv_plugin(str(tmp_path), cuda_graph="no")
+    npt = a.nx * a.nz
+    rng = np.random.default_rng(5)
+    for it in range(3):
+        ra = a.compute_gradient()
+        rb = b.compute_gradient()
+        assert ra[1] == rb[1] and ra[1] > 0  # misfit
+        for k in ("k_lam_f64", "k_mu_f64"):
+            assert torch.equal(getattr(a, k), getattr(b, k)), (it, k)
+        assert np.array_equal(ra[0], rb[0])  # smoothed kernel
+        assert len(a._graphs) == 1 and not getattr(b, "_graphs", None)
+        new_mu = ((2600.0 * 1732.0 ** 2) * (1 + 0.01 * (it + 1) * rng.standard_normal(npt))).astype(np.float32)
+        a.update_model(new_mu)
+        b.update_model(new_mu)
+    a.import_model(0)
+    assert not a._graphs
