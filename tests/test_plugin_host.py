@@ -172,3 +172,38 @@ def test_max_tail_bytes_is_the_longest_tail_that_fits():
             assert t2 == 0
     assert max_tail_bytes(nt, FWI_PSV, ns, g, 1e9, nrec) == 0  # nothing fits: no tail
     assert max_tail_bytes(100, FWI_PSV, 1, Grid(8, 8, 1.0, 1.0), 1e12, 0) == 100 * 5 * 4 * 8 * 8
+
+
+def test_gradient_graph_key():
+    """The kept gradient graph is reused only while the shots, the model's
+    and time functions' device buffers and the step settings are the same;
+    no graph with cuda_graph = no or a batch-memory cap."""
+    from types import SimpleNamespace
+    s = b200()
+    s.config = dict(combine_sources="no")
+    s.batch_memory, s.nt, s.dt, s.tile, s.kernel_rho = 0.0, 100, 1e-3, 0, False
+    t = lambda: torch.zeros(4)  # noqa: E731
+    s.model = SimpleNamespace(rho=t(), lam=t(), mu=t(), bound=t(), buo=t())
+    s.stf_x, s.stf_y, s.stf_z = t(), t(), t()
+    s.src_id, s.rec_id = np.array([3, 7], np.int32), np.array([1, 2, 5], np.int32)
+    k = s._graph_key(1, [0, 1])
+    assert k is not None and k == s._graph_key(1, [0, 1])
+    assert s._graph_key(1, [1]) != k  # other shots
+    s.model.mu.add_(1.0)  # values change in place: same buffers, same graph
+    assert s._graph_key(1, [0, 1]) == k
+    s.model.mu = t()  # a new buffer
+    assert s._graph_key(1, [0, 1]) != k
+    k = s._graph_key(1, [0, 1])
+    s.kernel_rho = True
+    assert s._graph_key(1, [0, 1]) != k
+    s.kernel_rho = False
+    s.rec_id = np.array([1, 2, 6], np.int32)
+    assert s._graph_key(1, [0, 1]) != k
+    s.batch_memory = 2.0 ** 30
+    assert s._graph_key(1, [0, 1]) is None
+    s.batch_memory = 0.0
+    s.config["cuda_graph"] = "no"
+    assert s._graph_key(1, [0, 1]) is None
+    s._graphs = {("x",): object()}
+    s._drop_graphs()
+    assert s._graphs == {}
