@@ -146,8 +146,8 @@ def config_of(a, w, extra=None, world=1):
                "checkpoints and stored steps ~150 GB: far above the 126 MB L2); no flush",
          "parallelism": "shots (contiguous blocks per rank, one FP64 all-reduce per gradient)"
                         if world > 1 else "shots", "gradient": a.gradient,
-         "step_overlap": bool(getattr(a, "step_overlap", 1)),
-         "cuda_graph": bool(getattr(a, "graph", 0)) and a.gradient == "exact"}
+         "step_overlap": bool(getattr(a, "step_overlap", 1)) and getattr(a, "impl", "b200") == "b200",
+         "cuda_graph": bool(getattr(a, "graph", 0)) and a.gradient == "exact" and getattr(a, "impl", "b200") == "b200"}
     if extra:
         c.update(extra)
     return c
