@@ -41,3 +41,19 @@ def test_config_counts_the_whole_job():
     assert c8["cells_per_step"] == 8 * c1["cells_per_step"]
     cs = bench.config_of(_args(shard=True), w, world=8)
     assert cs["shots"] == 32 and cs["shots_per_rank"] == 4 and cs["cells_per_step"] == c1["cells_per_step"]
+
+
+def test_config_names_the_launch_modes():
+    """The line says whether the value comes from the graph-replayed
+    gradient and whether the steps launch early; the CPU reference arm uses
+    neither."""
+    import bench
+    w = bench.workload(_args())
+    c = bench.config_of(_args(impl="b200", graph=1, step_overlap=1), w)
+    assert c["cuda_graph"] is True and c["step_overlap"] is True
+    c = bench.config_of(_args(impl="b200", graph=0, step_overlap=0), w)
+    assert c["cuda_graph"] is False and c["step_overlap"] is False
+    c = bench.config_of(_args(impl="b200", graph=1, gradient="reference"), w)
+    assert c["cuda_graph"] is False  # the continuous-adjoint path is launched step by step
+    c = bench.config_of(_args(impl="reference", graph=1, step_overlap=1), w)
+    assert c["cuda_graph"] is False and c["step_overlap"] is False
