@@ -296,12 +296,14 @@ class b200:
         k_rho_f64; returns the misfit (sum of per-shot, per-component norms).
 
         With all shots in one batch (the default when they fit), the first
-        call computes the gradient eagerly and then captures it in a CUDA
-        graph (seispie_b200.adjoint.GradientGraph) that it keeps with the
-        batch's buffers; later calls with the same shots, model buffers and
-        settings upload the observed traces into the graph's input buffers
-        and replay it: one launch per gradient, the same values bit for bit.
-        Any other call drops the kept graph first."""
+        call computes the gradient step by step and then captures it in CUDA
+        graphs (seispie_b200.adjoint.GradientGraph: the forward sweep; the
+        misfit step and the backward) that it keeps with the batch's
+        buffers; later calls with the same shots, model buffers and settings
+        replay them, uploading the observed traces into the graphs' input
+        buffers while the forward sweep runs: two launches per gradient, the
+        same values bit for bit.  Any other call drops the kept graphs
+        first."""
         from ..adjoint import ExactAdjoint, GradientGraph, max_tail_bytes
         key = self._graph_key(mode, shots)
         kept = self.__dict__.setdefault("_graphs", {})
