@@ -33,7 +33,7 @@ with N: weak scaling); ``--shard`` splits the 32 shots over the ranks
 
 Prints one JSON line (rank 0).  ``value`` is measured with every input in HBM,
 on the exact gradient captured once in a CUDA graph and replayed per step
-(seispie_b200.adjoint.GradientGraph: one host launch per gradient; the
+(seispie_b200.adjoint.GradientGraph: two host launches per gradient; the
 all-reduce and the smoothing run eagerly); ``eager`` holds the same gradient
 launched step by step, whose CUDA events time the roofline's kernel
 (``--graph 0`` makes the step-by-step gradient the value);
@@ -101,8 +101,8 @@ def parse():
                     help="1: programmatic dependent launch between the steps of a time loop that has the GPU to "
                          "itself (the forward sweep; the overlapped backward's streams never use it); 0: none")
     ap.add_argument("--graph", type=int, default=1, choices=[0, 1],
-                    help="1: value is the exact gradient captured in one CUDA graph (forward sweep, misfit and "
-                         "backward replayed as one launch per gradient; the step-by-step gradients that carry the "
+                    help="1: value is the exact gradient captured in CUDA graphs (forward sweep; misfit and "
+                         "backward) replayed as two launches per gradient (the step-by-step gradients that carry the "
                          "roofline's events are reported under 'eager'); 0: value is the step-by-step gradient")
     ap.add_argument("--shard", action="store_true",
                     help="split the --shots shots over the ranks (strong scaling) instead of --shots per rank")
@@ -473,8 +473,8 @@ def main():
     value = cells / (ms * 1e-3) / 1e9
     misfit_total = float(mis.item())
 
-    # The headline: the same gradient captured in one CUDA graph (forward sweep, misfit, backward) and
-    # replayed, one launch per gradient from the host; the eager gradients above, launched step by step,
+    # The headline: the same gradient captured in CUDA graphs (forward sweep; misfit and backward) and
+    # replayed, two launches per gradient from the host; the eager gradients above, launched step by step,
     # carry the per-launch CUDA events of the roofline.
     eager = None
     if a.gradient == "exact" and a.graph:
